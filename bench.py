@@ -1,0 +1,444 @@
+"""Benchmark: seconds to solve the 3D punched-lattice recovery on B200.
+
+One step = one complete interior-point solve (csipm_solve) of the workload,
+from A^T z0 to beta on the device.  Workload (default): 320^3 grid, 0.5%
+log-normal(0,1) nonzeros with random signs, balls of radius 3 punched on a
+period-16 lattice (~3% missing), sigma = 0.01, lambda = 0.05 ||A^T y||_inf,
+seeded synthetic data (the reference's crystallography volumes are not
+available).  Multi-GPU: one independent replica per rank (weak scaling, no
+collective on the path); times are the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload 3d320|3d256|2d1024|1d16384] [--precision fp64|mixed]
+
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "compressedsensingipm.jl_b200")
+sys.path.insert(0, PKG)
+
+WORKLOADS = {
+    "3d320": dict(kind="3d", dims=(320, 320, 320)),
+    "3d256": dict(kind="3d", dims=(256, 256, 256)),
+    "2d1024": dict(kind="2d", dims=(1024, 1024)),
+    "1d16384": dict(kind="1d", dims=(16384,)),
+}
+METRIC = "s-to-solve 3D 320^3 (beta 1e-6 vs FP64)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="3d320", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, wl):
+    return {
+        "workload": f"{wl['kind']}-{'x'.join(map(str, wl['dims']))}-punched-{args.precision}",
+        "grid": list(wl["dims"]),
+        "precision": args.precision,
+        "generator": "seeded synthetic (numpy default_rng), rank r uses seed r",
+        "missing": {"3d": "balls r=3 on a period-16 lattice", "2d": "disks r=4 period 32 + 5% random",
+                    "1d": "20 random gaps, 15%"}[wl["kind"]],
+        "lambda": {"3d": "0.05*||A^T y||_inf", "2d": "0.1*||A^T y||_inf", "1d": "0.1*||A^T y||_inf"}[wl["kind"]],
+        "stop": "relative LASSO duality gap 1e-8 (or scaled KKT error 1e-8)",
+        "l2": "no flush needed: the solve streams a multi-GB working set (> 126 MB L2) every CG iteration",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+# ----------------------------------------------------------------------- dist
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Dist:
+    def __init__(self, world, rank, local, use_gpu=True):
+        self.world, self.rank, self.local = world, rank, local
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            backend = "nccl" if use_gpu else "gloo"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device="cuda" if self.dist.get_backend() == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/csipm_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------- problem
+def build_problem(wl, seed):
+    """Seeded problem, synthesised with the library's own (unmasked) operator."""
+    import torch
+    import csipm
+    import csipm.problems as P
+    spec = P.make_spec(wl["kind"], dims=wl["dims"], seed=seed)
+    N = spec.N
+    zeros = torch.zeros(N, dtype=torch.float64, device="cuda")
+    op_full = csipm.FFTOperator(csipm.FFTParameters(len(spec.size), spec.size, zeros, 0.0, None))
+    x = op_full.M_perp_beta(torch.tensor(spec.beta_true, device="cuda")).cpu().numpy()
+    keep = spec.keep
+    z0 = np.where(keep, x + spec.noise, 0.0)
+    b = op_full.M_perpt_z(torch.tensor(z0, device="cuda"))
+    lam = float(spec.lam_factor * b.abs().max().item())
+    op_full.close()
+    del zeros, b
+    missing = np.flatnonzero(~keep).astype(np.int64)
+    return spec, z0, lam, missing
+
+
+# ----------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import csipm
+    from csipm import _native
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    D = Dist(world, rank, local)
+    wl = WORKLOADS[args.workload]
+    spec, z0_host, lam, missing = build_problem(wl, seed=rank)
+    N = spec.N
+    L = csipm.lib()
+
+    # resident problem
+    z0_dev = torch.tensor(z0_host, device="cuda")
+    params = csipm.FFTParameters(len(spec.size), spec.size, z0_dev, lam, missing)
+    nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision)
+    stream = torch.cuda.current_stream()
+    sol = torch.empty(2 * N, dtype=torch.float64, device="cuda")
+    st = _native.Stats()
+
+    def solve():
+        s = L.csipm_solve(nlp.handle, ctypes.c_void_p(sol.data_ptr()), ctypes.c_void_p(sol.data_ptr() + 8 * N),
+                          ctypes.byref(st))
+        if s != 0:
+            _native.check(s, nlp.handle)
+        return st.as_dict()
+
+    for _ in range(args.warmup):
+        solve()
+    stats = []
+    clocks = ClockSampler(local)
+    D.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        stats.append(solve())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    D.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = D.max(ms)
+    last = stats[-1]
+
+    # ---- end to end through the C ABI with host buffers (pinned), per step:
+    # H2D z0, csipm_create (mask from host indices, plans, A^T z0), csipm_solve,
+    # D2H beta, csipm_destroy
+    z0_pin = torch.tensor(z0_host).pin_memory()
+    beta_pin = torch.empty(N, dtype=torch.float64).pin_memory()
+    z0_e2e = torch.empty(N, dtype=torch.float64, device="cuda")
+    sol_e2e = torch.empty(2 * N, dtype=torch.float64, device="cuda")
+    miss = np.ascontiguousarray(missing)
+
+    def e2e_step():
+        z0_e2e.copy_(z0_pin, non_blocking=True)
+        prob = _native.Problem()
+        prob.dim = len(spec.size)
+        for d in range(3):
+            prob.size[d] = spec.size[d] if d < len(spec.size) else 1
+        prob.lam = lam
+        prob.z0 = z0_e2e.data_ptr()
+        prob.host_missing = miss.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        prob.n_missing = int(miss.size)
+        opt = csipm._options(rdft=True, precision=args.precision)
+        h = ctypes.c_void_p()
+        _native.check(L.csipm_create(ctypes.byref(prob), ctypes.byref(opt), ctypes.byref(h)))
+        s2 = _native.Stats()
+        _native.check(L.csipm_solve(h, ctypes.c_void_p(sol_e2e.data_ptr()), None, ctypes.byref(s2)), h)
+        beta_pin.copy_(sol_e2e[:N], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        L.csipm_destroy(h)
+
+    e2e_step()   # warm
+    D.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = D.max(e0.elapsed_time(e1) / args.steps)
+
+    # ---- roofline of the dominant kernel (each pass timed alone, CUDA events)
+    ms_p = (ctypes.c_double * 8)()
+    by_p = (ctypes.c_double * 8)()
+    names = ctypes.create_string_buffer(8 * 32)
+    npass = ctypes.c_int()
+    xr = torch.randn(N, dtype=torch.float64, device="cuda")
+    _native.check(L.csipm_profile_passes(nlp.handle, ctypes.c_void_p(xr.data_ptr()), 10, ms_p, by_p, names,
+                                         ctypes.byref(npass)), nlp.handle)
+    passes = []
+    for k in range(npass.value):
+        nm = names.raw[32 * k:32 * k + 32].split(b"\0")[0].decode()
+        passes.append({"kernel": nm, "ms": ms_p[k], "bytes": by_p[k], "GBps": by_p[k] / ms_p[k] / 1e6})
+    dom = max(passes, key=lambda p: p["ms"])
+    peak, peak_kind = measured_peaks()
+    matvec_ms = sum(p["ms"] for p in passes)
+    matvec_bytes = sum(p["bytes"] for p in passes)
+    roofline = {
+        "bound": "hbm",
+        "kernel": dom["kernel"],
+        "achieved": round(dom["GBps"], 1),
+        "peak": peak,
+        "peak_kind": f"{peak_kind} (burst copy, kernel timed alone)",
+        "unit": "GB/s",
+        "frac": round(dom["GBps"] / peak, 4),
+        "traffic": ncu_traffic(args.workload),
+        "algorithmic_bytes_per_launch": dom["bytes"],
+        "matvec": {"ms": round(matvec_ms, 4), "GBps": round(matvec_bytes / matvec_ms / 1e6, 1),
+                   "frac": round(matvec_bytes / matvec_ms / 1e6 / peak, 4)},
+        "passes": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in p.items()} for p in passes],
+    }
+
+    launches = int(last["launches"]) * args.steps
+    out = {
+        "metric": METRIC if args.workload == "3d320" else f"s-to-solve {args.workload}",
+        "value": round(ms / 1000.0, 5),
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32-matvec/f64-ipm",
+        "data": "synthetic",
+        "config": workload_config(args, wl),
+        "e2e": {"value": round(e2e_ms / 1000.0, 5), "unit": "s", "h2d_bytes_per_step": int(8 * N + 8 * miss.size),
+                "d2h_bytes_per_step": int(8 * N),
+                "includes": "H2D z0 + csipm_create (mask, plans, A^T z0) + csipm_solve + D2H beta + destroy"},
+        "solve": {"ipm_iter": last["ipm_iter"], "cg_iter": last["cg_iter"], "matvecs": last["matvecs"],
+                  "gap": last["gap"], "obj": last["obj"], "status": last["status"]},
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(spec, z0_host, lam, last)
+    D.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------- CPU baseline (oracle)
+def _cpu_sample(size, keep, z0, lam, reps):
+    """Times the oracle's FP64 A^T A and one Schur-CG vector update on the full grid."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    op = O.Operator(size, keep, True, workers=cores)
+    b = op.At(z0)
+    x = np.random.default_rng(0).standard_normal(b.size)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        q = op.AtA(x)
+    t_mv = (time.perf_counter() - t0) / reps
+    Db = np.abs(x)
+    Minv = 1.0 / (1.0 + Db)
+    r = b.copy()
+    p = Minv * r
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        q = q + Db * p
+        pq = p @ q
+        x += (1.0 / pq) * p
+        r -= (1.0 / pq) * q
+        rz = r @ (Minv * r)
+        p = Minv * r + rz * p
+    t_vec = (time.perf_counter() - t0) / reps
+    return t_mv, t_vec, cores
+
+
+def cpu_baseline(spec, z0, lam, stats):
+    t_mv, t_vec, cores = _cpu_sample(spec.size, spec.keep, z0, lam, reps=2)
+    est = stats["matvecs"] * t_mv + stats["cg_iter"] * t_vec
+    return {"value": round(est, 2), "unit": "s", "cores": cores, "kind": "port",
+            "sample": (f"oracle FP64 (numpy + scipy.fft pocketfft, workers={cores}) on the full grid: 2 A^T A "
+                       f"products ({t_mv:.2f} s each) and 2 CG vector updates ({t_vec:.2f} s each), scaled by "
+                       f"this solve's {stats['matvecs']} products and {stats['cg_iter']} CG iterations "
+                       f"(the CPU twin runs the same iteration counts)")}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import oracle_ipm as OI
+    import csipm.problems as P
+    cores = os.cpu_count() or 1
+    # iteration counts from a full CPU solve of a reduced instance of the same generator
+    small = tuple(max(2, (d // 5) // 2 * 2) for d in wl["dims"]) if wl["kind"] == "3d" else wl["dims"]
+    sspec = P.make_spec(wl["kind"], dims=small, seed=0)
+    op0 = O.Operator(sspec.size, None, True, workers=cores)
+    sprob = P.finalize(sspec, op0.A, op0.At)
+    sop = O.Operator(sspec.size, sspec.keep, True, workers=cores)
+    sb = sop.At(sprob.z0)
+    sop.n_matvec = 0
+    _, _, info = OI.ipm(sop, sb, sprob.lam, float(sprob.z0 @ sprob.z0), tol=1e-8)
+    counts = {"matvecs": sop.n_matvec, "cg_iter": info["cg_iter"], "ipm_iter": info["ipm_iter"]}
+    spec = P.make_spec(wl["kind"], dims=wl["dims"], seed=0)
+    opf = O.Operator(spec.size, None, True, workers=cores)
+    prob = P.finalize(spec, opf.A, opf.At)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        t_mv, t_vec, _ = _cpu_sample(spec.size, spec.keep, prob.z0, prob.lam, reps=1)
+        if s >= args.warmup:
+            vals.append(counts["matvecs"] * t_mv + counts["cg_iter"] * t_vec)
+    v = float(np.mean(vals))
+    sample = (f"CPU FP64 port of the path (numpy + scipy.fft pocketfft, workers={cores}); per step one A^T A "
+              f"product and one CG vector update timed on the full {'x'.join(map(str, wl['dims']))} grid, scaled by "
+              f"the iteration counts of a full CPU solve of the same generator at {'x'.join(map(str, small))} "
+              f"({counts['ipm_iter']} IPM iterations, {counts['cg_iter']} CG iterations, {counts['matvecs']} products)")
+    out = {
+        "impl": "reference",
+        "metric": METRIC if args.workload == "3d320" else f"s-to-solve {args.workload}",
+        "value": round(v, 3),
+        "unit": "s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(v * 1000, 1),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": workload_config(args, wl),
+        "cpu_baseline": {"value": round(v, 3), "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

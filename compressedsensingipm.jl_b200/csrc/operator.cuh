@@ -1,0 +1,520 @@
+// The masked sampling operator A = P_Omega * sqrt(N) * Re(IDFT(B .)) and its
+// adjoint, applied matrix-free through fused real-FFT passes.
+//
+// Layout in HBM: one half spectrum (M1+1) x N2 x N3 of complex values, dim 1
+// fastest, pitch ld1; the mask as one bit per real sample, rows of N1 bits
+// padded to 32-bit words.  Pass structure (3D; 2D drops the dim-3 passes, 1D is
+// a single row pass):
+//
+//   A^T A x :  [gather x -> inverse FFT dim 3] -> [inverse dim 2]
+//              -> [row: C2R dim 1, scale, mask, R2C dim 1]
+//              -> [forward dim 2] -> [forward dim 3 -> scatter + epilogue]
+//
+// The beta -> spectrum gather is fused into the first pass and the
+// spectrum -> beta scatter (plus any elementwise epilogue, e.g. the CG's
+// q = A^T A p + D p and p.q) into the last, so beta-space vectors are touched
+// once per product and the real-space samples never reach HBM.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <set>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cplx.cuh"
+#include "fft_device.cuh"
+#include "geometry.h"
+#include "plan.h"
+#include "reduce.cuh"
+
+namespace csipm {
+
+enum PassIn { IN_SPEC = 0, IN_GATHER = 1, IN_REAL = 2 };
+enum PassOut { OUT_SPEC = 0, OUT_SCATTER = 1, OUT_REAL = 2 };
+
+constexpr double SQRT2_D = 1.4142135623730951;
+
+template <typename T>
+struct PassArgs {
+    Geom g;
+    FftPlanDev pl;
+    const cplx_t<T>* tw;     // Ltab-th roots of unity (global memory)
+    int Ltab;
+    int tw_in_smem;
+    cplx_t<T>* spec;
+    // strided passes
+    int n_lines;             // number of dim-1 positions (M1+1)
+    long long so, sx;        // element strides of the outer index and of the transform index
+    int jk_mode;             // 0: (j,k) = (o,x)   1: (j,k) = (x,o)   2: (j,k) = (x,0)
+    // row passes
+    int nrows, rb, tbp;
+    const uint32_t* maskw;
+    int wpr;
+    double scale;
+    const T* real_in;
+    T* real_out;
+    const int* skip;         // when non-null and *skip != 0 the pass returns at once (converged CG)
+};
+
+// ------------------------------------------------------------- epilogues
+template <typename TO>
+struct EpiStore {
+    TO* out;
+    __device__ __forceinline__ void put(int l, double v) { out[l] = (TO)v; }
+    __device__ __forceinline__ void finish() {}
+};
+
+// q = A^T A p + D .* p, accumulating p.q (CG product)
+template <typename TV>
+struct EpiCG {
+    const TV* p;
+    const TV* D;
+    TV* q;
+    RedWorkspace ws;
+    double acc;
+    __device__ __forceinline__ void put(int l, double v) {
+        const double pv = (double)p[l];
+        const TV qv = (TV)(v + (double)D[l] * pv);
+        q[l] = qv;
+        acc += pv * (double)qv;
+    }
+    __device__ __forceinline__ void finish() {
+        double a[1] = {acc};
+        grid_reduce<1>(a, ws, 0u, 0u);
+    }
+};
+
+// ------------------------------------------------------- gather / scatter
+template <typename T, typename TS>
+__device__ __forceinline__ cplx_t<T> gather_val(const MapEntry& e, const TS* __restrict__ src) {
+    if (e.kind == KIND_VERT) return mk((T)src[e.re], (T)0);
+    const T r = (T)0.7071067811865476;   // 1/sqrt(2) (the operator is tolerance-checked, not bitwise)
+    const T a = (T)src[e.re], b = (T)src[e.im];
+    return e.kind == KIND_PLUS ? mk(a * r, b * r) : mk(a * r, -b * r);
+}
+
+template <typename T, class Epi>
+__device__ __forceinline__ void scatter_val(const MapEntry& e, cplx_t<T> v, Epi& ep) {
+    if (!e.src) return;
+    if (e.kind == KIND_VERT) {
+        ep.put(e.re, (double)v.x);
+    } else {
+        ep.put(e.re, SQRT2_D * (double)v.x);
+        ep.put(e.im, (e.kind == KIND_PLUS ? SQRT2_D : -SQRT2_D) * (double)v.y);
+    }
+}
+
+__device__ __forceinline__ void jk_of(int mode, int o, int x, int& j, int& k) {
+    if (mode == 0) { j = o; k = x; }
+    else if (mode == 1) { j = x; k = o; }
+    else { j = x; k = 0; }
+}
+
+// ------------------------------------------------------------ strided pass
+template <typename T, int TB, bool INV, int IN, int OUT, typename TS, class Epi>
+__global__ void __launch_bounds__(512) strided_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    using C = cplx_t<T>;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int L = a.pl.L;
+    __shared__ int s_rad[FFT_MAX_STAGES];
+    load_radices(a.pl, s_rad);
+    C* alt = buf + (size_t)L * TB;
+    const C* tw = a.tw;
+    if (a.tw_in_smem) {
+        C* tws = buf + (size_t)2 * L * TB;
+        for (int e = threadIdx.x; e < a.Ltab; e += blockDim.x) tws[e] = a.tw[e];
+        tw = tws;
+    }
+    const int i0 = blockIdx.x * TB;
+    const int o = blockIdx.y;
+    const int nb = min(TB, a.n_lines - i0);
+    const long long base = i0 + (long long)o * a.so;
+    for (int e = threadIdx.x; e < L * TB; e += blockDim.x) {
+        const int x = e / TB, b = e % TB;
+        C val = mk((T)0, (T)0);
+        if (b < nb) {
+            if (IN == IN_SPEC) {
+                val = a.spec[base + b + (long long)x * a.sx];
+            } else {
+                int j, k;
+                jk_of(a.jk_mode, o, x, j, k);
+                val = gather_val<T>(decode(a.g, i0 + b, j, k), src);
+            }
+        }
+        buf[e] = val;
+    }
+    __syncthreads();
+    const C* res = fft_lines<T, INV, true>(buf, alt, s_rad, a.pl.nst, L, TB, TB, tw, a.Ltab);
+    Epi ep = epi;
+    for (int e = threadIdx.x; e < L * TB; e += blockDim.x) {
+        const int x = e / TB, b = e % TB;
+        if (b < nb) {
+            if (OUT == OUT_SPEC) {
+                a.spec[base + b + (long long)x * a.sx] = res[e];
+            } else {
+                int j, k;
+                jk_of(a.jk_mode, o, x, j, k);
+                scatter_val<T>(decode(a.g, i0 + b, j, k), res[e], ep);
+            }
+        }
+    }
+    if (OUT == OUT_SCATTER) ep.finish();
+}
+
+// ---------------------------------------------------------------- row pass
+// Z[k] = (X[k] + conj X[M-k]) + i conj(W^k) (X[k] - conj X[M-k])   (C2R pre-processing)
+template <typename C>
+__device__ __forceinline__ C c2r_pre(C xa, C xb, C w) {
+    C s = cadd(xa, cconj(xb)), d = csub(xa, cconj(xb));
+    return cadd(s, cmul_i(cmulc(d, w)));
+}
+// X[k] = (Z[k] + conj Z[M-k]) - i W^k (Z[k] - conj Z[M-k])            (R2C post-processing)
+template <typename C>
+__device__ __forceinline__ C r2c_post(C za, C zb, C w) {
+    C s = cadd(za, cconj(zb)), d = csub(za, cconj(zb));
+    return csub(s, cmul_i(cmul(d, w)));
+}
+
+template <typename T, int IN, int OUT, bool MASK, bool PP, typename TS, class Epi>
+__global__ void __launch_bounds__(PP ? 512 : 1024) row_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    using C = cplx_t<T>;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int M = a.g.m1;
+    const int RB = a.rb, TBP = a.tbp;
+    __shared__ int s_rad[FFT_MAX_STAGES];
+    load_radices(a.pl, s_rad);
+    const size_t span = (size_t)(M + 1) * TBP;
+    C* alt = PP ? buf + span : nullptr;
+    const C* tw = a.tw;
+    if (a.tw_in_smem) {
+        C* tws = buf + (PP ? 2 : 1) * span;
+        for (int e = threadIdx.x; e < a.Ltab; e += blockDim.x) tws[e] = a.tw[e];
+        tw = tws;
+    }
+    const int r0 = blockIdx.x * RB;
+    const int nr = min(RB, a.nrows - r0);
+    const C zero = mk((T)0, (T)0);
+
+    // ---- load
+    if (IN == IN_REAL) {
+        for (int e = threadIdx.x; e < M * RB; e += blockDim.x) {
+            const int b = e / M, n = e % M;
+            C val = zero;
+            if (b < nr) val = *reinterpret_cast<const C*>(a.real_in + (size_t)(r0 + b) * a.g.n1 + 2 * n);
+            buf[n * TBP + b] = val;
+        }
+    } else {
+        for (int e = threadIdx.x; e < (M + 1) * RB; e += blockDim.x) {
+            const int b = e / (M + 1), n = e % (M + 1);
+            C val = zero;
+            if (b < nr) {
+                if (IN == IN_SPEC) val = a.spec[(size_t)(r0 + b) * a.g.ld1 + n];
+                else val = gather_val<T>(decode1(a.g, n), src);
+            }
+            buf[n * TBP + b] = val;
+        }
+    }
+    __syncthreads();
+    const int half = M / 2;
+    C* cur = buf;
+    if (IN != IN_REAL) {
+        for (int e = threadIdx.x; e < (half + 1) * RB; e += blockDim.x) {
+            const int b = e % RB, k = e / RB;
+            if (k == 0) {
+                const C x0 = buf[b], xm = buf[M * TBP + b];
+                buf[b] = c2r_pre(x0, xm, tw[0]);
+            } else if (2 * k == M) {
+                const C xk = buf[k * TBP + b];
+                buf[k * TBP + b] = c2r_pre(xk, xk, tw[k]);
+            } else {
+                const C xk = buf[k * TBP + b], xm = buf[(M - k) * TBP + b];
+                buf[k * TBP + b] = c2r_pre(xk, xm, tw[k]);
+                buf[(M - k) * TBP + b] = c2r_pre(xm, xk, tw[M - k]);
+            }
+        }
+        __syncthreads();
+        cur = fft_lines<T, true, PP>(buf, alt, s_rad, a.pl.nst, M, RB, TBP, tw, a.Ltab);
+    }
+    // ---- middle: scale and mask the real samples (x[2n], x[2n+1]) = (Re z[n], Im z[n])
+    const T sc = (T)a.scale;
+    for (int e = threadIdx.x; e < M * RB; e += blockDim.x) {
+        const int b = e / M, n = e % M;
+        if (b < nr) {
+            C y = cur[n * TBP + b];
+            y.x *= sc;
+            y.y *= sc;
+            if (MASK) {
+                const uint32_t w = a.maskw[(size_t)(r0 + b) * a.wpr + (n >> 4)];
+                const int sh = (2 * n) & 31;
+                if (!((w >> sh) & 1u)) y.x = (T)0;
+                if (!((w >> (sh + 1)) & 1u)) y.y = (T)0;
+            }
+            if (OUT == OUT_REAL) *reinterpret_cast<C*>(a.real_out + (size_t)(r0 + b) * a.g.n1 + 2 * n) = y;
+            else cur[n * TBP + b] = y;
+        }
+    }
+    if (OUT == OUT_REAL) return;
+    __syncthreads();
+    C* other = PP ? (cur == buf ? alt : buf) : nullptr;
+    cur = fft_lines<T, false, PP>(cur, other, s_rad, a.pl.nst, M, RB, TBP, tw, a.Ltab);
+    buf = cur;
+    for (int e = threadIdx.x; e < (half + 1) * RB; e += blockDim.x) {
+        const int b = e % RB, k = e / RB;
+        if (k == 0) {
+            const C z0 = buf[b];
+            buf[b] = r2c_post(z0, z0, tw[0]);
+            buf[M * TBP + b] = mk((T)2 * (z0.x - z0.y), (T)0);
+        } else if (2 * k == M) {
+            const C zk = buf[k * TBP + b];
+            buf[k * TBP + b] = r2c_post(zk, zk, tw[k]);
+        } else {
+            const C zk = buf[k * TBP + b], zm = buf[(M - k) * TBP + b];
+            buf[k * TBP + b] = r2c_post(zk, zm, tw[k]);
+            buf[(M - k) * TBP + b] = r2c_post(zm, zk, tw[M - k]);
+        }
+    }
+    __syncthreads();
+    if (OUT == OUT_SPEC) {
+        for (int e = threadIdx.x; e < (M + 1) * RB; e += blockDim.x) {
+            const int b = e / (M + 1), n = e % (M + 1);
+            if (b < nr) a.spec[(size_t)(r0 + b) * a.g.ld1 + n] = buf[n * TBP + b];
+        }
+    } else {
+        Epi ep = epi;
+        for (int n = threadIdx.x; n <= M; n += blockDim.x) scatter_val<T>(decode1(a.g, n), buf[n * TBP], ep);
+        ep.finish();
+    }
+}
+
+// ------------------------------------------------------------ host side
+struct PassCfg {
+    int tb = 0;          // lines per CTA (strided) / rows per CTA (row pass)
+    int tbp = 0;         // padded line stride in shared memory
+    int threads = 0;
+    size_t smem = 0;
+    int tw_in_smem = 0;
+    int pp = 1;          // 1: double-buffered (ping-pong) stages, 0: in place
+    dim3 grid;
+};
+
+template <typename T>
+class FftOperator {
+public:
+    using C = cplx_t<T>;
+    Geom g{};
+    cudaStream_t stream = nullptr;
+    C* spec = nullptr;              // (m1+1) x n2 x n3, pitch ld1
+    uint32_t* maskw = nullptr;      // nullptr: no missing samples
+    int wpr = 0;
+    FftPlanDev plan1{}, plan2{}, plan3{};
+    C* tw1 = nullptr;               // n1-th roots (row pass)
+    C* tw2 = nullptr;
+    C* tw3 = nullptr;
+    PassCfg row_cfg, s2_cfg, s3_cfg;
+    size_t bytes = 0;
+
+    ~FftOperator() { release(); }
+
+    void release() {
+        cudaFree(spec); spec = nullptr;
+        cudaFree(maskw); maskw = nullptr;
+        cudaFree(tw1); tw1 = nullptr;
+        cudaFree(tw2); tw2 = nullptr;
+        cudaFree(tw3); tw3 = nullptr;
+    }
+
+    static bool upload_table(int L, C** dst, std::string* err) {
+        std::vector<double> t;
+        twiddle_table(L, &t);
+        std::vector<C> h(L);
+        for (int e = 0; e < L; ++e) h[e] = mk((T)t[2 * e], (T)t[2 * e + 1]);
+        if (cudaMalloc(dst, sizeof(C) * L) != cudaSuccess) { *err = "out of device memory (twiddles)"; return false; }
+        cudaMemcpy(*dst, h.data(), sizeof(C) * L, cudaMemcpyHostToDevice);
+        return true;
+    }
+
+    // conservative dynamic shared-memory budget per CTA (B200 opt-in limit is 227 KB incl. static)
+    static size_t smem_limit() { return 200 * 1024; }
+
+    // Strided passes always double-buffer: TB lines of L elements, twice.
+    bool choose_strided(const FftPlanDev& pl, int Ltab, int n_lines, int n_outer, PassCfg* cfg, std::string* err) {
+        const int L = pl.L;
+        const int cands[4] = {sizeof(T) == 8 ? 8 : 16, sizeof(T) == 8 ? 4 : 8, sizeof(T) == 8 ? 2 : 4, 2};
+        for (int tb : cands) {
+            const size_t data = 2 * (size_t)L * tb * sizeof(C);
+            if (data > smem_limit()) continue;
+            int thr = ((L * tb) / 4 + 31) / 32 * 32;
+            thr = std::max(64, std::min(512, thr));
+            cfg->tb = tb;
+            cfg->tbp = tb;
+            cfg->threads = thr;
+            cfg->pp = 1;
+            const size_t tws = (size_t)Ltab * sizeof(C);
+            cfg->tw_in_smem = (data + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
+            cfg->smem = data + (cfg->tw_in_smem ? tws : 0);
+            cfg->grid = dim3((n_lines + tb - 1) / tb, n_outer, 1);
+            return true;
+        }
+        *err = "transform length too large for the on-chip strided pass";
+        return false;
+    }
+
+    // Row passes double-buffer when two copies fit in shared memory, else they
+    // run in place with the register-staged stages.
+    bool choose_row(int nrows, PassCfg* cfg, std::string* err) {
+        const int M = g.m1;
+        const int Ltab = g.n1;
+        const size_t tws = (size_t)Ltab * sizeof(C);
+        int rb = 1;
+        while (rb < 16 && rb * 2 <= nrows && (size_t)(M + 1) * (rb * 2 + 1) * sizeof(C) <= 24 * 1024) rb *= 2;
+        for (; rb >= 1; rb /= 2) {
+            const int tbp = rb > 1 ? rb + 1 : 1;
+            const size_t one = (size_t)(M + 1) * tbp * sizeof(C);
+            if (2 * one <= smem_limit()) {
+                int thr = ((M * rb) / 4 + 31) / 32 * 32;
+                thr = std::max(64, std::min(512, thr));
+                cfg->pp = 1;
+                cfg->tb = rb;
+                cfg->tbp = tbp;
+                cfg->threads = thr;
+                cfg->tw_in_smem = (2 * one + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
+                cfg->smem = 2 * one + (cfg->tw_in_smem ? tws : 0);
+                cfg->grid = dim3((nrows + rb - 1) / rb, 1, 1);
+                return true;
+            }
+            if (one > smem_limit()) continue;
+            int thr = ((M * rb + 7) / 8 + 31) / 32 * 32;
+            thr = std::max(64, std::min(1024, thr));
+            while (thr < 1024 && !plan_fits(plan1, rb, thr)) thr += 32;
+            if (!plan_fits(plan1, rb, thr)) continue;
+            cfg->pp = 0;
+            cfg->tb = rb;
+            cfg->tbp = tbp;
+            cfg->threads = thr;
+            cfg->tw_in_smem = (one + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
+            cfg->smem = one + (cfg->tw_in_smem ? tws : 0);
+            cfg->grid = dim3((nrows + rb - 1) / rb, 1, 1);
+            return true;
+        }
+        *err = "dimension 1 too large for the on-chip row pass";
+        return false;
+    }
+
+    // host_keep: N bytes (1 = observed) or nullptr for no mask
+    bool init(const Geom& geom, const uint8_t* host_keep, cudaStream_t st, std::string* err) {
+        g = geom;
+        stream = st;
+        if (!make_fft_plan(g.m1, &plan1, err)) return false;
+        if (g.dim >= 2 && !make_fft_plan(g.n2, &plan2, err)) return false;
+        if (g.dim >= 3 && !make_fft_plan(g.n3, &plan3, err)) return false;
+        const int nrows = g.n2 * g.n3;
+        if (!choose_row(nrows, &row_cfg, err)) return false;
+        if (g.dim >= 2 && !choose_strided(plan2, g.n2, g.m1 + 1, g.dim == 3 ? g.n3 : 1, &s2_cfg, err)) return false;
+        if (g.dim >= 3 && !choose_strided(plan3, g.n3, g.m1 + 1, g.n2, &s3_cfg, err)) return false;
+        if (!upload_table(g.n1, &tw1, err)) return false;
+        if (g.dim >= 2 && !upload_table(g.n2, &tw2, err)) return false;
+        if (g.dim >= 3 && !upload_table(g.n3, &tw3, err)) return false;
+        const size_t spec_elems = (size_t)g.ld1 * g.n2 * g.n3;
+        if (cudaMalloc(&spec, sizeof(C) * spec_elems) != cudaSuccess) { *err = "out of device memory (spectrum)"; return false; }
+        bytes += sizeof(C) * spec_elems;
+        if (host_keep) {
+            wpr = (g.n1 + 31) / 32;
+            std::vector<uint32_t> w((size_t)wpr * nrows, 0u);
+            for (int r = 0; r < nrows; ++r)
+                for (int i = 0; i < g.n1; ++i)
+                    if (host_keep[(size_t)r * g.n1 + i]) w[(size_t)r * wpr + (i >> 5)] |= 1u << (i & 31);
+            if (cudaMalloc(&maskw, sizeof(uint32_t) * w.size()) != cudaSuccess) { *err = "out of device memory (mask)"; return false; }
+            cudaMemcpy(maskw, w.data(), sizeof(uint32_t) * w.size(), cudaMemcpyHostToDevice);
+            bytes += sizeof(uint32_t) * w.size();
+        }
+        return true;
+    }
+
+    PassArgs<T> row_args(double scale, const T* real_in, T* real_out) const {
+        PassArgs<T> a{};
+        a.g = g; a.pl = plan1; a.tw = tw1; a.Ltab = g.n1; a.tw_in_smem = row_cfg.tw_in_smem;
+        a.spec = spec; a.nrows = g.n2 * g.n3; a.rb = row_cfg.tb; a.tbp = row_cfg.tbp;
+        a.maskw = maskw; a.wpr = wpr; a.scale = scale; a.real_in = real_in; a.real_out = real_out;
+        return a;
+    }
+    // axis 2 or 3
+    PassArgs<T> strided_args(int axis) const {
+        PassArgs<T> a{};
+        a.g = g;
+        a.spec = spec;
+        a.n_lines = g.m1 + 1;
+        if (axis == 3) {
+            a.pl = plan3; a.tw = tw3; a.Ltab = g.n3; a.tw_in_smem = s3_cfg.tw_in_smem;
+            a.so = g.ld1; a.sx = (long long)g.ld1 * g.n2; a.jk_mode = 0;
+        } else {
+            a.pl = plan2; a.tw = tw2; a.Ltab = g.n2; a.tw_in_smem = s2_cfg.tw_in_smem;
+            a.so = (long long)g.ld1 * g.n2; a.sx = g.ld1; a.jk_mode = g.dim == 3 ? 1 : 2;
+        }
+        return a;
+    }
+};
+
+// Opt a kernel into the large dynamic shared-memory carve-out once per
+// (kernel, device).
+inline bool smem_optin_needed(const void* fn, int dev) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lk(mu);
+    return done.insert({fn, dev}).second;
+}
+
+// The opt-in covers dynamic + static shared memory, so the dynamic limit set
+// here is the device's per-block opt-in maximum minus the kernel's static part.
+template <typename K>
+inline cudaError_t smem_optin(K kernel, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!smem_optin_needed((const void*)kernel, dev)) return cudaSuccess;
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if ((size_t)dyn < smem) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
+
+// Launch helpers (template dispatch on TB).
+template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
+inline cudaError_t launch_strided(const PassCfg& c, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    switch (c.tb) {
+#define CSIPM_TB_CASE(TBV)                                                                            \
+        case TBV: {                                                                                   \
+            auto k = strided_pass_kernel<T, TBV, INV, IN, OUT, TS, Epi>;                              \
+            e = smem_optin(k, c.smem);                                                                \
+            if (e != cudaSuccess) return e;                                                           \
+            k<<<c.grid, c.threads, c.smem, st>>>(a, src, epi);                                        \
+        } break;
+        CSIPM_TB_CASE(2) CSIPM_TB_CASE(4) CSIPM_TB_CASE(8) CSIPM_TB_CASE(16)
+#undef CSIPM_TB_CASE
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
+inline cudaError_t launch_row(const PassCfg& c, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
+    auto k = c.pp ? row_pass_kernel<T, IN, OUT, MASK, true, TS, Epi> : row_pass_kernel<T, IN, OUT, MASK, false, TS, Epi>;
+    cudaError_t e = smem_optin(k, c.smem);
+    if (e != cudaSuccess) return e;
+    k<<<c.grid, c.threads, c.smem, st>>>(a, src, epi);
+    return cudaGetLastError();
+}
+
+}  // namespace csipm

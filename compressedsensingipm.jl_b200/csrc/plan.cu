@@ -1,0 +1,99 @@
+#include "plan.h"
+
+#include <cmath>
+
+namespace csipm {
+
+bool make_fft_plan(int L, FftPlanDev* out, std::string* err) {
+    FftPlanDev p{};
+    p.L = L;
+    p.nst = 0;
+    if (L < 1) {
+        if (err) *err = "FFT length must be positive";
+        return false;
+    }
+    int r = L;
+    int twos = 0;
+    while (r % 2 == 0) { r /= 2; ++twos; }
+    auto push = [&](int radix) -> bool {
+        if (p.nst >= FFT_MAX_STAGES) return false;
+        p.rad[p.nst++] = radix;
+        return true;
+    };
+    // 2^twos = 8^a * {1, 4*4 (for 2^4 -> 16 when rem 1), 4 (rem 2)} ; a lone 2 only for L=2
+    int rem = twos % 3, a = twos / 3;
+    if (rem == 1 && a >= 1) { a -= 1; rem = 4; }   // 8*2 -> 4*4
+    for (int i = 0; i < a; ++i) if (!push(8)) goto too_many;
+    if (rem == 1) { if (!push(2)) goto too_many; }
+    else if (rem == 2) { if (!push(4)) goto too_many; }
+    else if (rem == 4) { if (!push(4) || !push(4)) goto too_many; }
+    for (int f : {5, 3, 7}) {
+        while (r % f == 0) { if (!push(f)) goto too_many; r /= f; }
+    }
+    for (int f = 11; r > 1; f += 2) {
+        while (r % f == 0) { if (!push(f)) goto too_many; r /= f; }
+        if ((long long)f * f > r && r > 1) { if (!push(r)) goto too_many; r = 1; }
+    }
+    *out = p;
+    return true;
+too_many:
+    if (err) *err = "FFT length has too many prime factors";
+    return false;
+}
+
+void twiddle_table(int L, std::vector<double>* re_im) {
+    re_im->resize(2 * (size_t)L);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int e = 0; e < L; ++e) {
+        // reduce to the first octant for accuracy, then rebuild by symmetry
+        long long num = e;               // angle = 2*pi*num/L
+        long double c, s;
+        // use exact rational symmetries: num/L in [0,1)
+        long long n8 = 8LL * num;        // octant index = floor(8*num/L)
+        int oct = (int)(n8 / L);
+        long double frac = (long double)(n8 - (long long)oct * L) / (long double)L;   // in [0,1)
+        long double th = frac * (twopi / 8.0L);                                         // [0, pi/4)
+        long double cs = cosl(th), sn = sinl(th);
+        // angle = oct*pi/4 + th ; build cos/sin of that
+        const long double h = 0.70710678118654752440084436210484903928L;
+        switch (oct) {
+            case 0: c = cs; s = sn; break;
+            case 1: c = h * (cs - sn); s = h * (cs + sn); break;
+            case 2: c = -sn; s = cs; break;
+            case 3: c = -h * (cs + sn); s = h * (cs - sn); break;
+            case 4: c = -cs; s = -sn; break;
+            case 5: c = -h * (cs - sn); s = -h * (cs + sn); break;
+            case 6: c = sn; s = -cs; break;
+            default: c = h * (cs + sn); s = -h * (cs - sn); break;
+        }
+        // for exact quarter/eighth points the reduction gives th = 0
+        (*re_im)[2 * (size_t)e] = (double)c;
+        (*re_im)[2 * (size_t)e + 1] = (double)(-s);   // exp(-i*angle)
+    }
+}
+
+bool plan_fits(const FftPlanDev& pl, int lines, int nthreads) {
+    const long long total = (long long)lines * pl.L;
+    for (int s = 0; s < pl.nst; ++s) {
+        const int R = pl.rad[s];
+        long long items;
+        long long cap;
+        switch (R) {
+            case 2: cap = MaxItems<2>::v; break;
+            case 3: cap = MaxItems<3>::v; break;
+            case 4: cap = MaxItems<4>::v; break;
+            case 5: cap = MaxItems<5>::v; break;
+            case 7: cap = MaxItems<7>::v; break;
+            case 8: cap = MaxItems<8>::v; break;
+            default: cap = GENERIC_MAX_ITEMS; break;
+        }
+        if (R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8)
+            items = (total / R + nthreads - 1) / nthreads;
+        else
+            items = (total + nthreads - 1) / nthreads;
+        if (items > cap) return false;
+    }
+    return true;
+}
+
+}  // namespace csipm

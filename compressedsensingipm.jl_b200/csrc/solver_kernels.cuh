@@ -1,0 +1,540 @@
+// Elementwise + reduction kernels of the interior-point solve, the fused PCG
+// and the MadNLP KKT-plugin products.  Every kernel is a grid-stride loop over
+// the N beta-space indices; reductions are deterministic (reduce.cuh).
+//
+// Formulation (src/fft_model.jl:20-34, 91-101): variables [beta; c], slacks
+// s1 = c + beta >= 0, s2 = c - beta >= 0 with multipliers z1, z2 >= 0.
+// Newton system condensed exactly as src/fft_kkt.jl does: with
+// D1 = z1/s1, D2 = z2/s2, L1 = D1 + D2, L2 = D1 - D2,
+//     [A'A + L1, L2; L2, L1] [db; dc] = [fb; fc]
+// and dc eliminated:  (A'A + Db) db = fb - L2 fc / L1,  Db = 4 D1 D2 / (D1 + D2),
+// preconditioned by 1/(1 + Db) — the Schur complement of the reference's
+// block preconditioner (src/fft_kkt.jl:46-85) on the same split.
+#pragma once
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "reduce.cuh"
+
+namespace csipm {
+
+#define CSIPM_GRID_LOOP(i, n) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+constexpr int EW_THREADS = 256;
+
+// ------------------------------------------------------------------ CG scalars
+// Device scalar block of one CG solve.  rz is double-buffered by iteration parity.
+struct CgScalars {
+    double rz[2];
+    double pq;
+    double thresh;      // stop when sqrt(rz) <= thresh
+    double rz0;
+    int done;           // 1: converged or broke down (later kernels of the solve return at once)
+    int iters;          // iterations completed
+    int breakdown;      // 1: p'q <= 0 or non-finite
+    int pad;
+};
+
+// r = rhs - q (q = (Q + D) x0 computed by the operator), or r = rhs when x0 == 0;
+// z = Minv r ; p = z ; rz = r.z ; thresh = atol + rtol*sqrt(rz)
+template <typename TV>
+__global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
+                               const TV* __restrict__ Minv, TV* __restrict__ r, TV* __restrict__ p,
+                               RedWorkspace ws, CgScalars* sc, double atol, double rtol) {
+    double acc[1] = {0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        double rv = rhs[i];
+        if (has_x0) rv -= (double)q[i];
+        const double zv = Minv ? (double)Minv[i] * rv : rv;
+        r[i] = (TV)rv;
+        p[i] = (TV)zv;
+        acc[0] += rv * zv;
+    }
+    if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
+        const double rz = ws.out[0];
+        sc->rz[0] = rz;
+        sc->rz0 = rz;
+        sc->thresh = atol + rtol * sqrt(rz);
+        sc->iters = 0;
+        sc->breakdown = 0;
+        sc->done = (sqrt(rz) <= sc->thresh) ? 1 : 0;
+        if (!isfinite(rz)) { sc->done = 1; sc->breakdown = 1; }
+    }
+}
+
+// alpha = rz/pq ; x += alpha p ; r -= alpha q ; rz' = r.(Minv r)
+template <typename TV, typename TX>
+__global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
+                                 const TV* __restrict__ q, const TV* __restrict__ Minv, RedWorkspace ws, CgScalars* sc) {
+    if (sc->done) return;
+    const double pq = sc->pq;
+    const double rz = sc->rz[it & 1];
+    const double alpha = rz / pq;
+    double acc[1] = {0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double pv = (double)p[i];
+        x[i] = (TX)((double)x[i] + alpha * pv);
+        const double rv = (double)r[i] - alpha * (double)q[i];
+        r[i] = (TV)rv;
+        acc[0] += Minv ? rv * (double)Minv[i] * rv : rv * rv;
+    }
+    if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
+        const double rzn = ws.out[0];
+        sc->rz[(it + 1) & 1] = rzn;
+        sc->iters = it + 1;
+        if (!(pq > 0.0) || !isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
+        else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
+    }
+}
+
+// p = Minv r + (rz'/rz) p
+template <typename TV>
+__global__ void cg_pupdate_kernel(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
+                                  const CgScalars* sc) {
+    if (sc->done) return;
+    const double b = sc->rz[(it + 1) & 1] / sc->rz[it & 1];
+    CSIPM_GRID_LOOP(i, n) {
+        const double zv = Minv ? (double)Minv[i] * (double)r[i] : (double)r[i];
+        p[i] = (TV)(zv + b * (double)p[i]);
+    }
+}
+
+// ------------------------------------------------------------------ IPM state
+// Reductions of the residual kernel (component index):
+enum { RR_SZ = 0, RR_BB, RR_BQB, RR_L1, RR_GINF, RR_RDINF, RR_RCINF, RR_SUMC, RR_N };
+constexpr unsigned RR_MAXMASK = (1u << RR_GINF) | (1u << RR_RDINF) | (1u << RR_RCINF);
+
+// beta = soft(b, lambda); reduce max|beta| and max|b|
+__global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
+                                 RedWorkspace ws) {
+    double acc[2] = {0.0, 0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double bi = b[i];
+        const double a = fabs(bi) - lam;
+        const double v = a > 0.0 ? copysign(a, bi) : 0.0;
+        beta[i] = v;
+        acc[0] = fmax(acc[0], fabs(v));
+        acc[1] = fmax(acc[1], fabs(bi));
+    }
+    grid_reduce<2>(acc, ws, 3u, 0u);
+}
+
+// Dual start from the clipped gradient with lz = max(lambda, 1e-3 |b|_inf, 1e-12)
+// (the floor keeps lambda = 0 interior); c = |beta| + mu0/min(z1,z2),
+// mu0 = 0.1*lz*max(1e-3, max|beta|).  mx = {max|beta|, max|b|}.
+__global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+                                 const double* __restrict__ beta, const double* __restrict__ mx,
+                                 double* __restrict__ c, double* __restrict__ z1, double* __restrict__ z2) {
+    const double lz = fmax(fmax(lam, 1e-3 * mx[1]), 1e-12);
+    const double mu0 = 0.1 * lz * fmax(1e-3, mx[0]);
+    CSIPM_GRID_LOOP(i, n) {
+        double g = Qb[i] - b[i];
+        g = fmin(fmax(g, -0.5 * lz), 0.5 * lz);
+        const double a = 0.5 * (lz + g), d = 0.5 * (lz - g);
+        z1[i] = a;
+        z2[i] = d;
+        c[i] = fabs(beta[i]) + mu0 / fmin(a, d);
+    }
+}
+
+// rd = Qb - b - z1 + z2 (stored) and the scalar diagnostics
+__global__ void ipm_residual_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+                                    const double* __restrict__ beta, const double* __restrict__ c,
+                                    const double* __restrict__ z1, const double* __restrict__ z2,
+                                    double* __restrict__ rd, RedWorkspace ws) {
+    double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i], q = Qb[i], bb = b[i];
+        const double s1 = ce + be, s2 = ce - be;
+        const double r = q - bb - a + d;
+        rd[i] = r;
+        const double rc = lam - a - d;
+        acc[RR_SZ] += s1 * a + s2 * d;
+        acc[RR_BB] += bb * be;
+        acc[RR_BQB] += be * q;
+        acc[RR_L1] += fabs(be);
+        acc[RR_GINF] = fmax(acc[RR_GINF], fabs(bb - q));
+        acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
+        acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
+        acc[RR_SUMC] += ce;
+    }
+    grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
+}
+
+// Barrier diagonals of the condensed Schur system: Db = 4 D1 D2/(D1 + D2), Minv = 1/(1 + Db)
+template <typename TV>
+__global__ void ipm_diag_kernel(long long n, const double* __restrict__ beta, const double* __restrict__ c,
+                                const double* __restrict__ z1, const double* __restrict__ z2,
+                                double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
+                                TV* __restrict__ Minv_lo, int precond) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = beta[i], ce = c[i];
+        const double D1 = z1[i] / (ce + be), D2 = z2[i] / (ce - be);
+        const double db = 4.0 * D1 * D2 / (D1 + D2);
+        const double mi = precond ? 1.0 / (1.0 + db) : 1.0;
+        Db[i] = db;
+        Minv[i] = mi;
+        if (Db_lo) { Db_lo[i] = (TV)db; Minv_lo[i] = (TV)mi; }
+    }
+}
+
+// Newton direction of one element given db, the centring target sigmu and the
+// second-order correction (cor1, cor2).
+struct ElemDir { double dc, ds1, ds2, dz1, dz2; };
+
+__device__ __forceinline__ ElemDir elem_direction(double be, double ce, double a, double d, double lam,
+                                                  double sigmu, double cor1, double cor2, double db) {
+    const double s1 = ce + be, s2 = ce - be;
+    const double D1 = a / s1, D2 = d / s2;
+    const double L1 = D1 + D2, L2 = D1 - D2;
+    const double h1 = (sigmu - s1 * a - cor1) / s1;
+    const double h2 = (sigmu - s2 * d - cor2) / s2;
+    const double rc = lam - a - d;
+    const double fc = -rc + h1 + h2;
+    ElemDir o;
+    o.dc = (fc - L2 * db) / L1;
+    o.ds1 = o.dc + db;
+    o.ds2 = o.dc - db;
+    o.dz1 = h1 - D1 * o.ds1;
+    o.dz2 = h2 - D2 * o.ds2;
+    return o;
+}
+
+// rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 ; corrector uses the affine direction dba
+__global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+                               const double* __restrict__ z1, const double* __restrict__ z2,
+                               const double* __restrict__ rd, const double* __restrict__ dba, double sigmu,
+                               double* __restrict__ rhs) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        double cor1 = 0.0, cor2 = 0.0;
+        if (dba) {
+            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            cor1 = f.ds1 * f.dz1;
+            cor2 = f.ds2 * f.dz2;
+        }
+        const double s1 = ce + be, s2 = ce - be;
+        const double D1 = a / s1, D2 = d / s2;
+        const double L1 = D1 + D2, L2 = D1 - D2;
+        const double h1 = (sigmu - s1 * a - cor1) / s1;
+        const double h2 = (sigmu - s2 * d - cor2) / s2;
+        const double fb = -rd[i] + h1 - h2;
+        const double fc = -(lam - a - d) + h1 + h2;
+        rhs[i] = fb - L2 * fc / L1;
+    }
+}
+
+// Step statistics of a direction: min ratios (primal, dual) and the sums for mu_aff.
+enum { SS_MINP = 0, SS_MIND, SS_SZ, SS_CROSS, SS_DD, SS_N };
+constexpr unsigned SS_MINMASK = (1u << SS_MINP) | (1u << SS_MIND);
+
+__global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+                                     const double* __restrict__ z1, const double* __restrict__ z2,
+                                     const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
+                                     RedWorkspace ws) {
+    double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        double cor1 = 0.0, cor2 = 0.0;
+        if (dba) {
+            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            cor1 = f.ds1 * f.dz1;
+            cor2 = f.ds2 * f.dz2;
+        }
+        const ElemDir o = elem_direction(be, ce, a, d, lam, sigmu, cor1, cor2, db[i]);
+        const double s1 = ce + be, s2 = ce - be;
+        if (o.ds1 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s1 / o.ds1);
+        if (o.ds2 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s2 / o.ds2);
+        if (o.dz1 < 0.0) acc[SS_MIND] = fmin(acc[SS_MIND], -a / o.dz1);
+        if (o.dz2 < 0.0) acc[SS_MIND] = fmin(acc[SS_MIND], -d / o.dz2);
+        acc[SS_SZ] += s1 * a + s2 * d;
+        acc[SS_CROSS] += s1 * o.dz1 + o.ds1 * a + s2 * o.dz2 + o.ds2 * d;
+        acc[SS_DD] += o.ds1 * o.dz1 + o.ds2 * o.dz2;
+    }
+    grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
+}
+
+// beta += ap db ; c += ap dc ; z += ad dz
+__global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ c,
+                                  double* __restrict__ z1, double* __restrict__ z2, const double* __restrict__ dba,
+                                  double sigmu, const double* __restrict__ db, double ap, double ad) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        double cor1 = 0.0, cor2 = 0.0;
+        if (dba) {
+            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            cor1 = f.ds1 * f.dz1;
+            cor2 = f.ds2 * f.dz2;
+        }
+        const double dbi = db[i];
+        const ElemDir o = elem_direction(be, ce, a, d, lam, sigmu, cor1, cor2, dbi);
+        beta[i] = be + ap * dbi;
+        c[i] = ce + ap * o.dc;
+        z1[i] = a + ad * o.dz1;
+        z2[i] = d + ad * o.dz2;
+    }
+}
+
+// ------------------------------------------------------------------ utilities
+template <typename TA, typename TB>
+__global__ void convert_kernel(long long n, const TA* __restrict__ a, TB* __restrict__ b) {
+    CSIPM_GRID_LOOP(i, n) b[i] = (TB)a[i];
+}
+
+__global__ void axpy_kernel(long long n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
+    CSIPM_GRID_LOOP(i, n) y[i] += alpha * x[i];
+}
+
+// y = x - y  (residual r = rhs - Kx in place on y)
+__global__ void sub_from_kernel(long long n, const double* __restrict__ x, double* __restrict__ y) {
+    CSIPM_GRID_LOOP(i, n) y[i] = x[i] - y[i];
+}
+
+// dot products on the device
+__global__ void dot2_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                            const double* __restrict__ c2, const double* __restrict__ d2, RedWorkspace ws) {
+    double acc[2] = {0.0, 0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        acc[0] += a[i] * b[i];
+        if (c2) acc[1] += c2[i] * d2[i];
+    }
+    grid_reduce<2>(acc, ws, 0u, 0u);
+}
+
+// ------------------------------------------------------------------ NLPModels / KKT plugin
+// g = [AtA beta - Atz0 ; lambda] (beta part fused in the operator epilogue)
+struct EpiGrad {
+    const double* b;
+    double* g;
+    __device__ __forceinline__ void put(int l, double v) { g[l] = v - b[l]; }
+    __device__ __forceinline__ void finish() {}
+};
+
+__global__ void fill_kernel(long long n, double v, double* __restrict__ y) {
+    CSIPM_GRID_LOOP(i, n) y[i] = v;
+}
+
+// cons!: c = [-beta - c ; beta - c]   (src/fft_model.jl:91-101)
+__global__ void cons_kernel(long long n, const double* __restrict__ x, double* __restrict__ out) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double be = x[i], ce = x[n + i];
+        out[i] = -be - ce;
+        out[n + i] = be - ce;
+    }
+}
+
+// hprod: hv = w [AtA v_b ; 0]
+struct EpiScale {
+    double w;
+    double* out;
+    __device__ __forceinline__ void put(int l, double v) { out[l] = w * v; }
+    __device__ __forceinline__ void finish() {}
+};
+
+// build_kkt!  (src/fft_kkt.jl:285-307)
+__global__ void kkt_build_kernel(long long n, const double* __restrict__ pr_diag, double* __restrict__ L1,
+                                 double* __restrict__ L2, double* __restrict__ P11, double* __restrict__ P12,
+                                 double* __restrict__ P22) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double S1 = pr_diag[2 * n + i], S2 = pr_diag[3 * n + i];
+        const double l1 = S1 + S2, l2 = S1 - S2;
+        const double Minv = 1.0 / (1.0 + l1);
+        const double S = 1.0 / (l1 - l2 * l2 * Minv);
+        L1[i] = l1;
+        L2[i] = l2;
+        P22[i] = S;
+        P12[i] = -l2 * S * Minv;
+        P11[i] = Minv + Minv * l2 * S * l2 * Minv;
+    }
+}
+
+// condensed mul!  yb = beta*yb + alpha*(AtA xb + L1 xb + L2 xz), yz = beta*yz + alpha*(L2 xb + L1 xz)
+// (src/fft_kkt.jl:27-44); the AtA part arrives through the operator epilogue.
+struct EpiCondensed {
+    const double* x;    // 2N
+    double* y;          // 2N
+    const double* L1;
+    const double* L2;
+    long long n;
+    double alpha, beta;
+    __device__ __forceinline__ void put(int l, double v) {
+        const double xb = x[l], xz = x[n + l];
+        const double l1 = L1[l], l2 = L2[l];
+        y[l] = beta * y[l] + alpha * (v + l1 * xb + l2 * xz);
+        y[n + l] = beta * y[n + l] + alpha * (l2 * xb + l1 * xz);
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+// preconditioner mul!  (src/fft_kkt.jl:73-85)
+__global__ void precond_mul_kernel(long long n, double* __restrict__ y, const double* __restrict__ x,
+                                   const double* __restrict__ P11, const double* __restrict__ P12,
+                                   const double* __restrict__ P22, double alpha, double beta) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double xb = x[i], xz = x[n + i];
+        y[i] = beta * y[i] + alpha * (P11[i] * xb + P12[i] * xz);
+        y[n + i] = beta * y[n + i] + alpha * (P12[i] * xb + P22[i] * xz);
+    }
+}
+
+// full KKT mul! body (src/fft_kkt.jl:223-246) fused into the operator epilogue
+struct EpiKKT {
+    const double* x;    // 6N
+    double* y;          // 6N
+    long long n;
+    double alpha, beta;
+    __device__ __forceinline__ void put(int l, double v) {
+        const long long N = n;
+        const double xb = x[l], xz = x[N + l], xs1 = x[2 * N + l], xs2 = x[3 * N + l];
+        const double xy1 = x[4 * N + l], xy2 = x[5 * N + l];
+        y[l] = beta * y[l] + alpha * (v - xy1 + xy2);
+        y[N + l] = beta * y[N + l] - alpha * (xy1 + xy2);
+        y[2 * N + l] = beta * y[2 * N + l] - alpha * xy1;
+        y[3 * N + l] = beta * y[3 * N + l] - alpha * xy2;
+        y[4 * N + l] = beta * y[4 * N + l] + alpha * (-xb - xz - xs1);
+        y[5 * N + l] = beta * y[5 * N + l] + alpha * (xb - xz - xs2);
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+// jtprod!  (src/fft_kkt.jl:253-275)
+__global__ void jtprod_kernel(long long n, double* __restrict__ y, const double* __restrict__ x) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double y1 = x[i], y2 = x[n + i];
+        y[i] = -y1 + y2;
+        y[n + i] = -y1 - y2;
+        y[2 * n + i] = -y1;
+        y[3 * n + i] = -y2;
+    }
+}
+
+// solve_kkt! right-hand side (src/fft_kkt.jl:334-335): b = [w1 - w3 + w4 - S1 w5 + S2 w6 ; w2 - w3 - w4 - S1 w5 - S2 w6]
+__global__ void kkt_rhs_kernel(long long n, const double* __restrict__ w, const double* __restrict__ pr_diag,
+                               double* __restrict__ b) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double S1 = pr_diag[2 * n + i], S2 = pr_diag[3 * n + i];
+        const double w1 = w[i], w2 = w[n + i], w3 = w[2 * n + i], w4 = w[3 * n + i], w5 = w[4 * n + i], w6 = w[5 * n + i];
+        b[i] = w1 - w3 + w4 - S1 * w5 + S2 * w6;
+        b[n + i] = w2 - w3 - w4 - S1 * w5 - S2 * w6;
+    }
+}
+
+// solve_kkt! back-substitution (src/fft_kkt.jl:345-350)
+__global__ void kkt_back_kernel(long long n, double* __restrict__ w, const double* __restrict__ x,
+                                const double* __restrict__ pr_diag) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double S1 = pr_diag[2 * n + i], S2 = pr_diag[3 * n + i];
+        const double w1 = x[i], w2 = x[n + i];
+        double w3 = w[2 * n + i], w4 = w[3 * n + i], w5 = w[4 * n + i], w6 = w[5 * n + i];
+        w5 = -(w3 + S1 * (w1 + w2 + w5));
+        w6 = -(w4 + S2 * (-w1 + w2 + w6));
+        w3 = (w3 + w5) / S1;
+        w4 = (w4 + w6) / S2;
+        w[i] = w1; w[n + i] = w2; w[2 * n + i] = w3; w[3 * n + i] = w4; w[4 * n + i] = w5; w[5 * n + i] = w6;
+    }
+}
+
+// ---- 2N PCG of the KKT plugin (Krylov.jl cg semantics, M = block preconditioner)
+// z = P r (2x2 blocks), written into z; returns r.z
+__device__ __forceinline__ void pblock(const double* P11, const double* P12, const double* P22, long long i,
+                                       double rb, double rz, double& zb, double& zz) {
+    if (P11) {
+        zb = P11[i] * rb + P12[i] * rz;
+        zz = P12[i] * rb + P22[i] * rz;
+    } else {
+        zb = rb;
+        zz = rz;
+    }
+}
+
+// x = 0, r = b, p = z = P r, rz = r.z
+__global__ void kcg_init_kernel(long long n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
+                                double* __restrict__ p, const double* __restrict__ P11, const double* __restrict__ P12,
+                                const double* __restrict__ P22, RedWorkspace ws, CgScalars* sc, double atol, double rtol) {
+    double acc[1] = {0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double rb = b[i], rzv = b[n + i];
+        double zb, zz;
+        pblock(P11, P12, P22, i, rb, rzv, zb, zz);
+        x[i] = 0.0; x[n + i] = 0.0;
+        r[i] = rb; r[n + i] = rzv;
+        p[i] = zb; p[n + i] = zz;
+        acc[0] += rb * zb + rzv * zz;
+    }
+    if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
+        const double rz = ws.out[0];
+        sc->rz[0] = rz;
+        sc->rz0 = rz;
+        sc->thresh = atol + rtol * sqrt(rz);
+        sc->iters = 0;
+        sc->breakdown = 0;
+        sc->done = (sqrt(rz) <= sc->thresh) ? 1 : 0;
+    }
+}
+
+// q = K p fused: qb = AtA pb + L1 pb + L2 pz ; qz = L2 pb + L1 pz ; acc p.q
+struct EpiKcg {
+    const double* p;
+    double* q;
+    const double* L1;
+    const double* L2;
+    long long n;
+    RedWorkspace ws;
+    double acc;
+    __device__ __forceinline__ void put(int l, double v) {
+        const double pb = p[l], pz = p[n + l];
+        const double l1 = L1[l], l2 = L2[l];
+        const double qb = v + l1 * pb + l2 * pz;
+        const double qz = l2 * pb + l1 * pz;
+        q[l] = qb;
+        q[n + l] = qz;
+        acc += pb * qb + pz * qz;
+    }
+    __device__ __forceinline__ void finish() {
+        double a[1] = {acc};
+        grid_reduce<1>(a, ws, 0u, 0u);
+    }
+};
+
+__global__ void kcg_update_kernel(long long n, int it, double* __restrict__ x, double* __restrict__ r,
+                                  const double* __restrict__ p, const double* __restrict__ q,
+                                  const double* __restrict__ P11, const double* __restrict__ P12,
+                                  const double* __restrict__ P22, RedWorkspace ws, CgScalars* sc) {
+    if (sc->done) return;
+    const double pq = sc->pq;
+    const double alpha = sc->rz[it & 1] / pq;
+    double acc[1] = {0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        x[i] += alpha * p[i];
+        x[n + i] += alpha * p[n + i];
+        const double rb = r[i] - alpha * q[i];
+        const double rzv = r[n + i] - alpha * q[n + i];
+        r[i] = rb;
+        r[n + i] = rzv;
+        double zb, zz;
+        pblock(P11, P12, P22, i, rb, rzv, zb, zz);
+        acc[0] += rb * zb + rzv * zz;
+    }
+    if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
+        const double rzn = ws.out[0];
+        sc->rz[(it + 1) & 1] = rzn;
+        sc->iters = it + 1;
+        if (!(pq > 0.0) || !isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
+        else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
+    }
+}
+
+__global__ void kcg_pupdate_kernel(long long n, int it, const double* __restrict__ r, double* __restrict__ p,
+                                   const double* __restrict__ P11, const double* __restrict__ P12,
+                                   const double* __restrict__ P22, const CgScalars* sc) {
+    if (sc->done) return;
+    const double b = sc->rz[(it + 1) & 1] / sc->rz[it & 1];
+    CSIPM_GRID_LOOP(i, n) {
+        double zb, zz;
+        pblock(P11, P12, P22, i, r[i], r[n + i], zb, zz);
+        p[i] = zb + b * p[i];
+        p[n + i] = zz + b * p[n + i];
+    }
+}
+
+}  // namespace csipm

@@ -1,0 +1,238 @@
+/*
+ * csipm.h — C ABI of the B200-native matrix-free interior-point hot path of
+ * CompressedSensingIPM.jl (sparse DFT recovery from a real signal with missing
+ * samples: min_beta 1/2 ||A beta - z0||^2 + lambda ||beta||_1,
+ * A = P_Omega * sqrt(N) * Re(IDFT(B beta))).
+ *
+ * Every entry point is the replacement for one function of the reference's
+ * NLPModels / MadNLP plugin surface; the reference location is given beside
+ * each declaration (paths inside the CompressedSensingIPM.jl repository).
+ *
+ * Conventions
+ *   - Arrays are column-major (dim 1 fastest) and 0-based, exactly Julia's
+ *     memory layout, so a CuArray's pointer can be passed unchanged.
+ *   - Vector arguments are DEVICE pointers owned by the caller (CuArray /
+ *     torch / cudaMalloc memory) unless the name says host_.  The library never
+ *     frees them.  Real arrays must be 16-byte aligned (CuArray/cudaMalloc
+ *     memory is; a view at an even element offset is).
+ *   - Complex arrays are interleaved (re, im) FP64, i.e. ComplexF64 memory.
+ *   - Every function returns a csipm_status (0 = success).  No exception
+ *     crosses the ABI; csipm_last_error() describes the last failure.
+ *   - One handle = one CUDA stream.  Calls are stream-ordered and asynchronous
+ *     except those returning a host scalar (csipm_obj, csipm_solve, ...),
+ *     which synchronise the handle's stream.  A handle is not thread-safe;
+ *     distinct handles may be used concurrently from different threads.
+ */
+#ifndef CSIPM_H
+#define CSIPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CSIPM_API __attribute__((visibility("default")))
+#else
+#define CSIPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSIPM_ABI_VERSION 1
+
+typedef enum {
+    CSIPM_OK = 0,
+    CSIPM_ERR_INVALID = -1,        /* bad argument (null pointer, size, misalignment) */
+    CSIPM_ERR_ODD_DIM = -2,        /* a dimension is odd or < 2 (src/fft_utils.jl:130 requires even sizes) */
+    CSIPM_ERR_UNSUPPORTED = -3,    /* size beyond the on-chip FFT passes */
+    CSIPM_ERR_OOM = -4,            /* device allocation failed */
+    CSIPM_ERR_CUDA = -5,           /* a CUDA call failed */
+    CSIPM_ERR_CG_MAXITER = -6,     /* CG hit its iteration cap before the tolerance */
+    CSIPM_ERR_NONFINITE = -7,      /* NaN/Inf detected in the iteration */
+    CSIPM_ERR_IPM_MAXITER = -8,    /* IPM hit max_iter before the tolerance */
+    CSIPM_ERR_NO_DEVICE = -9       /* no CUDA device / the library was not built for it */
+} csipm_status;
+
+typedef enum { CSIPM_FP64 = 0, CSIPM_MIXED = 1 } csipm_precision;
+
+typedef struct csipm_handle_s* csipm_handle;
+
+/* Problem description.  Replaces FFTParameters (src/fft_utils.jl:1-14). */
+typedef struct {
+    int dim;                        /* 1, 2 or 3                                 (DFTdim)  */
+    int size[3];                    /* N1, N2, N3 (unused entries ignored), even (DFTsize) */
+    double lambda;                  /* l1 weight                                 (lambda)  */
+    const double* z0;               /* DEVICE, N reals, zero at missing samples  (z0)      */
+    const int64_t* host_missing;    /* HOST, 0-based column-major linear indices of the
+                                       missing samples (index_missing, 1-based in Julia),
+                                       may be NULL when n_missing == 0 */
+    int64_t n_missing;
+} csipm_problem;
+
+/* Options.  Mirrors the FFTNLPModel kwargs (src/fft_model.jl:12-15) and the
+ * MadNLP options used by the reference drivers (test/ipm_example_1D.jl:60-70). */
+typedef struct {
+    int rdft;                  /* 1: real FFT / half spectrum (reference rdft=true); 0: full spectrum */
+    int precision;             /* csipm_precision */
+    int preconditioner;        /* 1: block-diagonal preconditioner (reference default true) */
+    double tol;                /* IPM stop: relative LASSO duality gap (reference tol=1e-8) */
+    int max_iter;              /* IPM iteration cap (reference max_iter=2000) */
+    double cg_atol;            /* KKT solve: CG absolute tolerance (reference atol=1e-12) */
+    double cg_rtol;            /* KKT solve: CG relative tolerance (reference rtol=0) */
+    int cg_maxit;              /* CG iteration cap per solve */
+    double ipm_cg_rtol;        /* csipm_solve: relative CG tolerance of each Newton solve */
+    int ir_max;                /* mixed precision: max FP64 refinement steps per Newton solve */
+    int verbose;               /* 1: print one line per IPM iteration to stderr */
+    void* stream;              /* cudaStream_t every call of the handle runs on; NULL: the default stream */
+} csipm_options;
+
+/* Per-solve statistics (MadNLPExecutionStats analogue + the reference's timers,
+ * src/fft_utils.jl:24-25, src/fft_kkt.jl:109-110). */
+typedef struct {
+    int status;                /* csipm_status of the solve */
+    int ipm_iter;              /* IPM iterations */
+    int cg_iter;               /* total CG iterations over all Newton solves */
+    int matvecs;               /* A^T A products (FP64 + FP32) */
+    int refinements;           /* FP64 iterative-refinement steps (mixed precision) */
+    double gap;                /* final relative LASSO duality gap */
+    double obj;                /* reference objective 1/2||A b||^2 - b'A^T z0 + lambda*sum(c) (src/fft_model.jl:66-75) */
+    double lasso_obj;          /* 1/2||A b - z0||^2 + lambda ||b||_1 */
+    double mu;                 /* final barrier parameter (average complementarity) */
+    double dual_inf;           /* final max |A^T A b - A^T z0 - z1 + z2| */
+    double solve_ms;           /* wall time of csipm_solve on the device stream */
+    long long launches;        /* kernels the solve launched (including early-exit CG tails) */
+} csipm_stats;
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* Fills `opt` with the reference defaults (rdft=1, FP64, preconditioner=1,
+ * tol=1e-8, max_iter=2000, cg_atol=1e-12, cg_rtol=0, cg_maxit=2N). */
+CSIPM_API int csipm_default_options(csipm_options* opt);
+
+/* Builds the operator, FFT plans, mask and workspaces and computes A^T z0.
+ * Replaces FFTOperator{VT}(...) (src/fft_utils.jl:16-54) together with the
+ * FFTNLPModel constructor (src/fft_model.jl:12-64) and create_kkt_system
+ * (src/fft_kkt.jl:113-156). */
+CSIPM_API int csipm_create(const csipm_problem* prob, const csipm_options* opt, csipm_handle* out);
+
+/* Frees everything the handle owns (never the caller's vectors). */
+CSIPM_API int csipm_destroy(csipm_handle h);
+
+/* Message of the last failure on `h` (or of the last failed csipm_create when h is NULL). */
+CSIPM_API const char* csipm_last_error(csipm_handle h);
+
+/* N = prod(size) and the device bytes the handle holds. */
+CSIPM_API int csipm_get_info(csipm_handle h, int64_t* n, size_t* device_bytes);
+
+/* Copies the cached A^T z0 (FFTNLPModel.M_perpt_z0, src/fft_model.jl:61-62) into out (N). */
+CSIPM_API int csipm_get_Atz0(csipm_handle h, double* out);
+
+/* ---------------------------------------------------------------- mapping */
+
+/* beta_to_DFT!(v, dim, size, beta; rdft) — src/fft_utils.jl:195-204
+ * (src/mapping_cuda.jl:114-365).  Bit-exact with src/mapping_cpu_kernels.jl.
+ * v: (N1/2+1)*N2*N3 complex when rdft=1, N1*N2*N3 complex when rdft=0. */
+CSIPM_API int csipm_beta_to_dft(int dim, const int* size, int rdft, const double* beta, double* v, void* stream);
+
+/* DFT_to_beta!(beta, dim, size, v) — src/fft_utils.jl:144-153
+ * (src/mapping_cuda.jl:1-111).  Reads only v[1:N1/2+1, :, :]; ld1 is the
+ * first-dimension extent of v (N1/2+1 for a half spectrum, N1 for a full one). */
+CSIPM_API int csipm_dft_to_beta(int dim, const int* size, int ld1, const double* v, double* beta, void* stream);
+
+/* ---------------------------------------------------------------- operator */
+
+/* M_perp_beta: x = P_Omega(sqrt(N) Re(ifft(B beta)))  — src/fft_utils.jl:95-117.  beta, x: N. */
+CSIPM_API int csipm_apply_A(csipm_handle h, const double* beta, double* x);
+
+/* M_perpt_z: beta = B^T(fft(z)/sqrt(N)), no mask  — src/fft_utils.jl:73-93.  z, beta: N. */
+CSIPM_API int csipm_apply_At(csipm_handle h, const double* z, double* beta);
+
+/* M_perpt_M_perp_vec: y = A^T A x  — src/fft_utils.jl:67-71, 119-123.  x, y: N. */
+CSIPM_API int csipm_apply_AtA(csipm_handle h, const double* x, double* y);
+
+/* ---------------------------------------------------------------- NLPModels */
+
+/* obj(nlp, x): 1/2||A beta||^2 - beta'A^T z0 + lambda*sum(c), x = [beta; c] (2N)
+ * — src/fft_model.jl:66-75.  Synchronises; *f is a host double. */
+CSIPM_API int csipm_obj(csipm_handle h, const double* x, double* f);
+
+/* grad!(nlp, x, g): g = [A^T A beta - A^T z0; lambda] — src/fft_model.jl:77-89.  x, g: 2N. */
+CSIPM_API int csipm_grad(csipm_handle h, const double* x, double* g);
+
+/* cons!(nlp, x, c): c = [-beta - c; beta - c] — src/fft_model.jl:91-101.  x, c: 2N. */
+CSIPM_API int csipm_cons(csipm_handle h, const double* x, double* c);
+
+/* Hessian-vector product of the Lagrangian (constraints are linear):
+ * hv = obj_weight * [A^T A v_beta; 0].  The reference sets hprod_available=false
+ * (src/fft_model.jl:55); the same product is the A^T A block of
+ * src/fft_kkt.jl:39-41.  v, hv: 2N. */
+CSIPM_API int csipm_hprod(csipm_handle h, const double* v, double* hv, double obj_weight);
+
+/* ---------------------------------------------------------------- KKT plugin */
+
+/* build_kkt!: Lambda1 = S1 + S2, Lambda2 = S1 - S2 and the preconditioner
+ * P11/P12/P22 from the slack block of pr_diag (S1 = pr_diag[2N:3N),
+ * S2 = pr_diag[3N:4N)) — src/fft_kkt.jl:285-307.  pr_diag: >= 4N. */
+CSIPM_API int csipm_kkt_build(csipm_handle h, const double* pr_diag);
+
+/* mul!(y, K, x, alpha, beta) with the condensed operator
+ * K = [A^T A + L1, L2; L2, L1] — src/fft_kkt.jl:27-44.  x, y: 2N. */
+CSIPM_API int csipm_condensed_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+
+/* mul!(y, P, x, alpha, beta) with the block-diagonal preconditioner
+ * — src/fft_kkt.jl:73-85.  x, y: 2N. */
+CSIPM_API int csipm_precond_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+
+/* Body of mul!(y::KKTVector, kkt, x, alpha, beta) — src/fft_kkt.jl:223-246:
+ * the 6N primal/slack/dual block [beta; c; s1; s2; y1; y2].  The caller adds
+ * MadNLP's _kktmul! diagonal terms (src/fft_kkt.jl:248) itself.  x, y: 6N. */
+CSIPM_API int csipm_kkt_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+
+/* jtprod!(y, kkt, x): y[0:4N) = J' x for the 2N constraint multipliers
+ * — src/fft_kkt.jl:253-275.  x: 2N, y: >= 4N. */
+CSIPM_API int csipm_jtprod(csipm_handle h, double* y, const double* x);
+
+/* Body of solve_kkt!(kkt, w) — src/fft_kkt.jl:316-350: right-hand side
+ * reduction, preconditioned CG on the condensed system (atol=cg_atol,
+ * rtol=cg_rtol), back-substitution, all in place on w = [w1..w6] (6N).  The
+ * caller runs MadNLP.reduce_rhs! before and finish_aug_solve! after
+ * (src/fft_kkt.jl:314, 352).  Requires a prior csipm_kkt_build with the same
+ * pr_diag.  *cg_iters receives the iteration count (Krylov iteration_count). */
+CSIPM_API int csipm_kkt_solve(csipm_handle h, double* w, const double* pr_diag, int* cg_iters);
+
+/* ---------------------------------------------------------------- solver */
+
+/* The whole interior-point solve on the device (ipm_solve!,
+ * src/CompressedSensingIPM.jl:31-36, with the MadNLP loop replaced by a
+ * primal-dual path-following method on the same formulation and the same
+ * condensed KKT operator).  beta_out (N) and, if non-NULL, c_out (N) receive
+ * the solution; stats may be NULL. */
+CSIPM_API int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* stats);
+
+/* ---------------------------------------------------------------- timers */
+
+/* Device time (ms, CUDA events) accumulated by the handle in the three buckets
+ * the reference keeps (fft_timer / mapping_timer, src/fft_utils.jl:24-25;
+ * krylov_timer, src/fft_kkt.jl:110): here operator products, elementwise
+ * IPM/mapping work and CG solves.  Reset with reset != 0. */
+CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elementwise_ms, double* krylov_ms, int reset);
+
+/* ---------------------------------------------------------------- diagnostics */
+
+/* Times each kernel of one A^T A product in isolation: every pass is launched
+ * `reps` times back to back between CUDA events on the handle's stream (the
+ * last pass with the CG epilogue q = A^T A p + D p, p.q).  Writes up to 8
+ * entries: ms_out[k] = average device ms per launch, bytes_out[k] = algorithmic
+ * HBM bytes per launch (each array read or written once), name_out (optional,
+ * 8 x 32 chars) = kernel role.  *npass receives the pass count (1, 3 or 5 for
+ * 1D/2D/3D).  x: N.  The reference keeps only host-side timers
+ * (src/fft_utils.jl:24-25); this has no counterpart there. */
+CSIPM_API int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_out, double* bytes_out,
+                                   char* name_out, int* npass);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSIPM_H */

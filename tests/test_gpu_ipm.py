@@ -1,0 +1,63 @@
+"""The device interior-point solve against the CPU twin (oracle_ipm) and the
+reference's known-answer checks."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import oracle_ipm as OI
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "known_answers.npz")
+
+
+@pytest.mark.parametrize("key", ["100", "200", "500", "16x16", "12x18", "16x24", "32x32", "8x8x8", "6x10x12",
+                                 "14x8x4", "8x6x4", "16x16x16"])
+@pytest.mark.parametrize("rdft", [True, False])
+def test_known_answer(cuda, key, rdft):
+    """test/ipm_example_{1,2,3}D.jl with check=true: no noise, no mask, lambda = 0,
+    ||beta_true - beta|| <= 1e-6 with beta_true = DFT_to_beta(fft(x)/sqrt(N))."""
+    import csipm
+    torch = cuda
+    g = np.load(GOLD)
+    size = tuple(int(s) for s in key.split("x"))
+    params = csipm.FFTParameters(len(size), size, torch.tensor(g["x_" + key], device="cuda"), 0.0, None)
+    nlp = csipm.FFTNLPModel(params, rdft=rdft)
+    res = csipm.ipm_solve(nlp)
+    assert res.status == 0, res.stats
+    assert np.linalg.norm(g["beta_" + key] - res.beta.cpu().numpy()) <= 1e-6
+
+
+def _problem(kind, dims, seed):
+    import csipm.problems as P
+    spec = P.make_spec(kind, dims=dims, seed=seed)
+    op0 = O.Operator(spec.size)
+    return P.finalize(spec, op0.A, op0.At)
+
+
+@pytest.mark.parametrize("kind,dims", [("1d", (2048,)), ("1d", (16384,)), ("2d", (64, 64)), ("2d", (128, 96)),
+                                       ("3d", (16, 16, 16)), ("3d", (32, 32, 32))])
+def test_parity_with_cpu_twin(cuda, kind, dims):
+    """Same seed, same algorithm: beta within 1e-6 relative, objective within
+    1e-8 relative, IPM iteration count within 1."""
+    import csipm
+    torch = cuda
+    prob = _problem(kind, dims, seed=1)
+    size = prob.size
+    params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+    nlp = csipm.FFTNLPModel(params, rdft=True, tol=1e-10)
+    res = csipm.ipm_solve(nlp)
+    assert res.status == 0, res.stats
+    op = O.Operator(size, prob.spec.keep)
+    b = op.At(prob.z0)
+    beta, c, info = OI.ipm(op, b, prob.lam, float(prob.z0 @ prob.z0), tol=1e-10)
+    assert info["status"] == "ok"
+    bg = res.beta.cpu().numpy()
+    assert np.linalg.norm(bg - beta) / np.linalg.norm(beta) <= 1e-6
+    Fg = OI.lasso_value(op, bg, prob.z0, prob.lam)
+    Fc = OI.lasso_value(op, beta, prob.z0, prob.lam)
+    assert abs(Fg - Fc) <= 1e-8 * Fc
+    assert abs(res.stats["ipm_iter"] - info["ipm_iter"]) <= 1
+    assert abs(res.stats["obj"] - info["obj"]) <= 1e-8 * abs(info["obj"])
