@@ -33,7 +33,7 @@ EXPORTS = (
     "csipm_get_Atz0", "csipm_beta_to_dft", "csipm_dft_to_beta", "csipm_apply_A", "csipm_apply_At",
     "csipm_apply_AtA", "csipm_obj", "csipm_grad", "csipm_cons", "csipm_hprod", "csipm_kkt_build",
     "csipm_condensed_mul", "csipm_precond_mul", "csipm_kkt_mul", "csipm_jtprod", "csipm_kkt_solve",
-    "csipm_solve", "csipm_get_timers", "csipm_profile_passes",
+    "csipm_solve", "csipm_get_timers", "csipm_profile_passes", "csipm_apply_AtA_static",
 )
 
 
@@ -126,6 +126,7 @@ def load(path: str | None = None):
         "csipm_solve": (I, [H, D, D, ctypes.POINTER(Stats)]),
         "csipm_get_timers": (I, [H, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.POINTER(dbl), I]),
         "csipm_profile_passes": (I, [H, D, I, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.c_char_p, ctypes.POINTER(I)]),
+        "csipm_apply_AtA_static": (I, [I, ctypes.POINTER(I), D, D, D, ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -103,6 +103,11 @@ bool valid_dims(int dim, const int* size, std::string* err, int* status) {
 
 }  // namespace
 
+namespace csipm {
+// lets other translation units report through csipm_last_error(NULL)
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace csipm
+
 // ====================================================================== handle
 struct csipm_handle_s {
     int device = 0;

@@ -319,10 +319,12 @@ public:
     C* tw3 = nullptr;
     PassCfg row_cfg, s2_cfg, s3_cfg;
     size_t bytes = 0;
+    bool owns = true;               // false: buffers belong to someone else; release() frees nothing
 
     ~FftOperator() { release(); }
 
     void release() {
+        if (!owns) return;
         cudaFree(spec); spec = nullptr;
         cudaFree(maskw); maskw = nullptr;
         cudaFree(tw1); tw1 = nullptr;

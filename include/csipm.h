@@ -218,6 +218,31 @@ CSIPM_API int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm
  * IPM/mapping work and CG solves.  Reset with reset != 0. */
 CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elementwise_ms, double* krylov_ms, int reset);
 
+/* ---------------------------------------------------------------- no allocation */
+
+/* y = A^T A x for callers that cannot allocate device memory.  No counterpart
+ * in the reference: it exists for callers whose device memory is owned by a
+ * pool they must not bypass (a Julia CUDA.jl or PyTorch process with a hard
+ * memory limit, a serving process that pre-commits all HBM to resident
+ * problems) and for loops that cannot afford cudaMalloc's implicit device
+ * synchronisation.  It calls no cudaMalloc, cudaFree or allocating library
+ * routine: its scratch (the half spectrum and the twiddle tables) lives in one
+ * file-scope device array of 32 MiB that every GPU loading the library holds
+ * until the process exits.  Problems whose half spectrum ((N1/2+1)*N2*N3
+ * complex values) and twiddle tables need more than 32 MiB — above about 2.09
+ * million complex values, e.g. 3D grids beyond 160^3 — are rejected with
+ * CSIPM_ERR_UNSUPPORTED and a message.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the array and each rewrites what it reads, so calls that overlap on the GPU
+ * race: serialise them (one stream, or events).  Inputs and outputs are the
+ * caller's: x, y (N, device), keep_bits (device, or NULL for no missing
+ * samples): one bit per sample, 1 = observed, column-major, LSB first, each
+ * dim-1 row of N1 bits padded to a whole number of 32-bit words.  Runs on
+ * `stream` (NULL: default stream); errors are reported by csipm_last_error(NULL). */
+CSIPM_API int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, const double* x, double* y,
+                                     void* stream);
+
 /* ---------------------------------------------------------------- diagnostics */
 
 /* Times each kernel of one A^T A product in isolation: every pass is launched
