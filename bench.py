@@ -9,7 +9,7 @@ available).  Multi-GPU: one independent replica per rank (weak scaling, no
 collective on the path); times are the max over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload 3d320|3d256|2d1024|1d16384] [--precision fp64|mixed]
+                    [--workload 3d320|3d256|3d160|3d128|2d1024|1d16384] [--precision fp64|mixed]
 
 Prints ONE JSON line on rank 0.
 """
@@ -33,6 +33,8 @@ sys.path.insert(0, PKG)
 WORKLOADS = {
     "3d320": dict(kind="3d", dims=(320, 320, 320)),
     "3d256": dict(kind="3d", dims=(256, 256, 256)),
+    "3d160": dict(kind="3d", dims=(160, 160, 160)),
+    "3d128": dict(kind="3d", dims=(128, 128, 128)),
     "2d1024": dict(kind="2d", dims=(1024, 1024)),
     "1d16384": dict(kind="1d", dims=(16384,)),
 }

@@ -18,6 +18,7 @@
 // other prime is done as a direct DFT.
 #pragma once
 #include "cplx.cuh"
+#include "roots.h"
 
 namespace csipm {
 
@@ -147,6 +148,53 @@ template <bool INV, typename T> struct Dft<7, INV, T> {
         }
     }
 };
+
+// Composite radix R = R1*R2 in registers: R2 DFTs of size R1 over
+// a[n2 + R2*n1], twiddles W_R^{n2*k1} (compile-time constants), then R1 DFTs
+// of size R2; output X[k1 + R1*k2].
+template <int R1, int R2, bool INV, typename T> struct DftComp {
+    using C = cplx_t<T>;
+    static constexpr int R = R1 * R2;
+    __device__ __forceinline__ static void run(C* a) {
+        C y[R];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) {
+            C t[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) t[n1] = a[n2 + R2 * n1];
+            Dft<R1, INV, T>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                const int m = (n2 * k1) % R;
+                C v = t[k1];
+                if (m != 0) {
+                    const C w = mk((T)RootTab<R>::re(m), (T)RootTab<R>::im(m));
+                    v = INV ? cmulc(v, w) : cmul(v, w);
+                }
+                y[k1 * R2 + n2] = v;
+            }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            C t[R2];
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) t[n2] = y[k1 * R2 + n2];
+            Dft<R2, INV, T>::run(t);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) a[k1 + R1 * k2] = t[k2];
+        }
+    }
+};
+
+template <bool INV, typename T> struct Dft<6, INV, T> : DftComp<2, 3, INV, T> {};
+template <bool INV, typename T> struct Dft<9, INV, T> : DftComp<3, 3, INV, T> {};
+template <bool INV, typename T> struct Dft<10, INV, T> : DftComp<2, 5, INV, T> {};
+template <bool INV, typename T> struct Dft<12, INV, T> : DftComp<4, 3, INV, T> {};
+template <bool INV, typename T> struct Dft<15, INV, T> : DftComp<3, 5, INV, T> {};
+template <bool INV, typename T> struct Dft<16, INV, T> : DftComp<4, 4, INV, T> {};
+template <bool INV, typename T> struct Dft<20, INV, T> : DftComp<4, 5, INV, T> {};
+template <bool INV, typename T> struct Dft<25, INV, T> : DftComp<5, 5, INV, T> {};
+template <bool INV, typename T> struct Dft<32, INV, T> : DftComp<8, 4, INV, T> {};
 
 // ------------------------------------------------------------------- stages
 template <typename T, int R, bool INV>
@@ -297,8 +345,17 @@ __device__ cplx_t<T>* fft_lines(cplx_t<T>* buf, cplx_t<T>* alt, const int* s_rad
                 case 3: stage_pp<T, 3, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
                 case 4: stage_pp<T, 4, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
                 case 5: stage_pp<T, 5, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 6: stage_pp<T, 6, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
                 case 7: stage_pp<T, 7, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
                 case 8: stage_pp<T, 8, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 9: stage_pp<T, 9, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 10: stage_pp<T, 10, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 12: stage_pp<T, 12, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 15: stage_pp<T, 15, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 16: stage_pp<T, 16, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 20: stage_pp<T, 20, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 25: stage_pp<T, 25, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
+                case 32: stage_pp<T, 32, INV>(in, out, L, TB, TBP, Ns, tw, step); break;
                 default: stage_generic_pp<T, INV>(in, out, L, TB, TBP, Ns, R, tw, step, Ltab); break;
             }
             __syncthreads();

@@ -1,0 +1,238 @@
+// Internal declarations shared by the library's translation units: the
+// handle, error plumbing, launch helpers and the operator dispatch (which
+// passes a product runs through for each dimension).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/csipm.h"
+#include "geometry.h"
+#include "operator.cuh"
+#include "solver_kernels.cuh"
+
+namespace csipm {
+void set_last_error(const std::string& msg);
+const char* get_last_error();
+}  // namespace csipm
+
+namespace csipm_internal {
+using namespace csipm;
+
+inline int ew_blocks(long long n) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    long long b = (n + EW_THREADS - 1) / EW_THREADS;
+    long long cap = (long long)sms * 8;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+inline bool valid_dims(int dim, const int* size, std::string* err, int* status) {
+    if (dim < 1 || dim > 3 || !size) { *err = "dim must be 1, 2 or 3"; *status = CSIPM_ERR_INVALID; return false; }
+    long long N = 1;
+    for (int d = 0; d < dim; ++d) {
+        if (size[d] < 2 || (size[d] % 2)) {
+            *err = "every dimension must be even and >= 2";
+            *status = CSIPM_ERR_ODD_DIM;
+            return false;
+        }
+        N *= size[d];
+    }
+    if (N >= (1LL << 31)) { *err = "N must be below 2^31"; *status = CSIPM_ERR_UNSUPPORTED; return false; }
+    return true;
+}
+
+}  // namespace csipm_internal
+
+using namespace csipm;
+using namespace csipm_internal;
+
+// ====================================================================== handle
+struct csipm_handle_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    csipm_options opt{};
+    Geom g{};
+    long long N = 0;
+    double lambda = 0.0;
+    double z0sq = 0.0;
+    FftOperator<double> op64;
+    std::string err;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    // reductions
+    double* partials = nullptr;
+    unsigned int* ticket = nullptr;
+    double* slots = nullptr;        // device scalar slots
+    double* hslots = nullptr;       // pinned host mirror
+    CgScalars* cgs = nullptr;       // device CG scalars
+    CgScalars* hcgs = nullptr;      // pinned host mirror
+
+    // model / IPM vectors (FP64)
+    double* b = nullptr;            // A^T z0
+    double *beta = nullptr, *c = nullptr, *z1 = nullptr, *z2 = nullptr, *Qb = nullptr, *rd = nullptr;
+    double *Db = nullptr, *Minv = nullptr, *rhs = nullptr, *dba = nullptr, *db = nullptr;
+    double *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr;
+    // KKT plugin (allocated on first use)
+    double *L1 = nullptr, *L2 = nullptr, *P11 = nullptr, *P12 = nullptr, *P22 = nullptr;
+    double *k_b = nullptr, *k_x = nullptr, *k_r = nullptr, *k_p = nullptr, *k_q = nullptr;
+
+    // counters / timers
+    int matvecs = 0;
+    long long launches = 0;
+    double krylov_ms = 0.0, total_ms = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~csipm_handle_s() {
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        op64.release();
+        if (hslots) cudaFreeHost(hslots);
+        if (hcgs) cudaFreeHost(hcgs);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    template <typename P>
+    bool alloc(P** p, size_t count) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, sizeof(P) * count) != cudaSuccess) {
+            err = "out of device memory";
+            return false;
+        }
+        allocs.push_back(q);
+        bytes += sizeof(P) * count;
+        *p = reinterpret_cast<P*>(q);
+        return true;
+    }
+
+    RedWorkspace ws(double* out) const { return RedWorkspace{partials, ticket, out}; }
+};
+
+namespace csipm_internal {
+
+
+inline int fail(csipm_handle h, int status, const std::string& msg) {
+    if (h) h->err = msg;
+    set_last_error(msg);
+    return status;
+}
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(h, CSIPM_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #call); \
+    } while (0)
+
+// slot indices in h->slots
+enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_COUNT = 64 };
+
+// ------------------------------------------------------------------ operator
+template <typename T, typename TS, class Epi>
+cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* skip, cudaStream_t st) {
+    const Geom& g = op.g;
+    const double sc = 1.0 / (2.0 * (double)g.N);
+    const bool mask = op.maskw != nullptr;
+    EpiStore<double> none{nullptr};
+    cudaError_t e;
+    PassArgs<T> ra = op.row_args(sc, nullptr, nullptr);
+    ra.skip = skip;
+    if (g.dim == 1) {
+        return mask ? launch_row<T, IN_GATHER, OUT_SCATTER, true>(op.row_cfg, ra, x, epi, st)
+                    : launch_row<T, IN_GATHER, OUT_SCATTER, false>(op.row_cfg, ra, x, epi, st);
+    }
+    if (g.dim == 2) {
+        PassArgs<T> a2 = op.strided_args(2);
+        a2.skip = skip;
+        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s2_cfg, a2, x, none, st);
+        if (e != cudaSuccess) return e;
+        e = mask ? launch_row<T, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
+                 : launch_row<T, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+        if (e != cudaSuccess) return e;
+        return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s2_cfg, a2, (const double*)nullptr, epi, st);
+    }
+    PassArgs<T> a3 = op.strided_args(3), a2 = op.strided_args(2);
+    a3.skip = skip;
+    a2.skip = skip;
+    e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s3_cfg, a3, x, none, st);
+    if (e != cudaSuccess) return e;
+    e = launch_strided<T, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st);
+    if (e != cudaSuccess) return e;
+    e = mask ? launch_row<T, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
+             : launch_row<T, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+    if (e != cudaSuccess) return e;
+    e = launch_strided<T, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st);
+    if (e != cudaSuccess) return e;
+    return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s3_cfg, a3, (const double*)nullptr, epi, st);
+}
+
+// x = P(sqrt(N) Re ifft(B beta))
+template <typename T, typename TS>
+cudaError_t op_A(FftOperator<T>& op, const TS* beta, T* x, cudaStream_t st) {
+    const Geom& g = op.g;
+    const bool mask = op.maskw != nullptr;
+    EpiStore<double> none{nullptr};
+    PassArgs<T> ra = op.row_args(1.0 / std::sqrt((double)g.N), nullptr, x);
+    cudaError_t e;
+    if (g.dim == 1)
+        return mask ? launch_row<T, IN_GATHER, OUT_REAL, true>(op.row_cfg, ra, beta, none, st)
+                    : launch_row<T, IN_GATHER, OUT_REAL, false>(op.row_cfg, ra, beta, none, st);
+    if (g.dim == 3) {
+        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s3_cfg, op.strided_args(3), beta, none, st);
+        if (e != cudaSuccess) return e;
+        e = launch_strided<T, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, none, st);
+    } else {
+        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s2_cfg, op.strided_args(2), beta, none, st);
+    }
+    if (e != cudaSuccess) return e;
+    return mask ? launch_row<T, IN_SPEC, OUT_REAL, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
+                : launch_row<T, IN_SPEC, OUT_REAL, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+}
+
+// beta = B^T(fft(z)/sqrt(N)) through the epilogue
+template <typename T, class Epi>
+cudaError_t op_At(FftOperator<T>& op, const T* z, const Epi& epi, cudaStream_t st) {
+    const Geom& g = op.g;
+    EpiStore<double> none{nullptr};
+    PassArgs<T> ra = op.row_args(1.0 / (2.0 * std::sqrt((double)g.N)), z, nullptr);
+    cudaError_t e;
+    if (g.dim == 1) return launch_row<T, IN_REAL, OUT_SCATTER, false>(op.row_cfg, ra, (const double*)nullptr, epi, st);
+    e = launch_row<T, IN_REAL, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+    if (e != cudaSuccess) return e;
+    if (g.dim == 2) return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, epi, st);
+    e = launch_strided<T, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, none, st);
+    if (e != cudaSuccess) return e;
+    return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s3_cfg, op.strided_args(3), (const double*)nullptr, epi, st);
+}
+
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+inline int passes_per_product(const Geom& g) { return g.dim == 3 ? 5 : (g.dim == 2 ? 3 : 1); }
+
+inline int read_slots(csipm_handle h, int first, int count) {
+    CK(cudaMemcpyAsync(h->hslots + first, h->slots + first, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CSIPM_OK;
+}
+
+
+int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
+int ensure_kkt_buffers(csipm_handle h);
+
+}  // namespace csipm_internal

@@ -97,9 +97,7 @@ int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, 
     op.g = g;
     op.stream = (cudaStream_t)stream;
     std::string err;
-    if (!make_fft_plan(g.m1, &op.plan1, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    if (dim >= 2 && !make_fft_plan(g.n2, &op.plan2, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    if (dim >= 3 && !make_fft_plan(g.n3, &op.plan3, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+    if (!op.make_plans(&err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
     if (!op.choose_row(g.n2 * g.n3, &op.row_cfg, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
     if (dim >= 2 && !op.choose_strided(op.plan2, g.n2, g.m1 + 1, dim == 3 ? g.n3 : 1, &op.s2_cfg, &err))
         return static_fail(CSIPM_ERR_UNSUPPORTED, err);

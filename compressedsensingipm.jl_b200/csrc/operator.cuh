@@ -18,7 +18,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <set>
 #include <string>
 #include <utility>
@@ -47,6 +49,7 @@ struct PassArgs {
     cplx_t<T>* spec;
     // strided passes
     int n_lines;             // number of dim-1 positions (M1+1)
+    int n_outer;             // number of lines per dim-1 position (outer index range)
     long long so, sx;        // element strides of the outer index and of the transform index
     int jk_mode;             // 0: (j,k) = (o,x)   1: (j,k) = (x,o)   2: (j,k) = (x,0)
     // row passes
@@ -59,11 +62,35 @@ struct PassArgs {
     const int* skip;         // when non-null and *skip != 0 the pass returns at once (converged CG)
 };
 
+// ------------------------------------------------------------- async copies
+// cp.async (LDGSTS): global -> shared without register staging, many in flight
+// per thread; completion is waited for with cp.async.wait_group (never spins).
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+template <int BYTES> __device__ __forceinline__ void cp_async(void* s, const void* g);
+template <> __device__ __forceinline__ void cp_async<16>(void* s, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+template <> __device__ __forceinline__ void cp_async<8>(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+template <> __device__ __forceinline__ void cp_async<4>(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ------------------------------------------------------------- epilogues
+// Two-phase epilogues: pre(l) loads what put(l, v, pre) needs, so a scatter
+// loop can issue the loads of several elements before it consumes them.
+struct NoPre {};
+
 template <typename TO>
 struct EpiStore {
     TO* out;
-    __device__ __forceinline__ void put(int l, double v) { out[l] = (TO)v; }
+    using Pre = NoPre;
+    __device__ __forceinline__ NoPre pre(int) const { return {}; }
+    __device__ __forceinline__ void put(int l, double v, const NoPre&) { out[l] = (TO)v; }
     __device__ __forceinline__ void finish() {}
 };
 
@@ -75,11 +102,12 @@ struct EpiCG {
     TV* q;
     RedWorkspace ws;
     double acc;
-    __device__ __forceinline__ void put(int l, double v) {
-        const double pv = (double)p[l];
-        const TV qv = (TV)(v + (double)D[l] * pv);
+    struct Pre { double p, d; };
+    __device__ __forceinline__ Pre pre(int l) const { return Pre{(double)p[l], (double)D[l]}; }
+    __device__ __forceinline__ void put(int l, double v, const Pre& r) {
+        const TV qv = (TV)(v + r.d * r.p);
         q[l] = qv;
-        acc += pv * (double)qv;
+        acc += r.p * (double)qv;
     }
     __device__ __forceinline__ void finish() {
         double a[1] = {acc};
@@ -96,14 +124,70 @@ __device__ __forceinline__ cplx_t<T> gather_val(const MapEntry& e, const TS* __r
     return e.kind == KIND_PLUS ? mk(a * r, b * r) : mk(a * r, -b * r);
 }
 
+// staged (re, im) of beta -> spectrum value, in place
+template <typename T>
+__device__ __forceinline__ cplx_t<T> gather_combine(const MapEntry& e, cplx_t<T> v) {
+    const T r = (T)0.7071067811865476;
+    if (e.kind == KIND_VERT) return mk(v.x, (T)0);
+    return e.kind == KIND_PLUS ? mk(v.x * r, v.y * r) : mk(v.x * r, -v.y * r);
+}
+
+// start the async copies of the two beta values of a spectrum position into its slot
+template <typename T, typename TS>
+__device__ __forceinline__ void gather_issue(const MapEntry& e, const TS* __restrict__ src, cplx_t<T>* slot) {
+    static_assert(sizeof(TS) == sizeof(T), "staged gather needs the source and spectrum precisions to match");
+    cp_async<sizeof(TS)>(&slot->x, src + e.re);
+    if (e.kind != KIND_VERT) cp_async<sizeof(TS)>(&slot->y, src + e.im);
+    else slot->y = (T)0;
+}
+
 template <typename T, class Epi>
-__device__ __forceinline__ void scatter_val(const MapEntry& e, cplx_t<T> v, Epi& ep) {
+__device__ __forceinline__ void scatter_one(const MapEntry& e, cplx_t<T> v, Epi& ep) {
     if (!e.src) return;
+    const typename Epi::Pre pr = ep.pre(e.re);
     if (e.kind == KIND_VERT) {
-        ep.put(e.re, (double)v.x);
+        ep.put(e.re, (double)v.x, pr);
     } else {
-        ep.put(e.re, SQRT2_D * (double)v.x);
-        ep.put(e.im, (e.kind == KIND_PLUS ? SQRT2_D : -SQRT2_D) * (double)v.y);
+        const typename Epi::Pre pi = ep.pre(e.im);
+        ep.put(e.re, SQRT2_D * (double)v.x, pr);
+        ep.put(e.im, (e.kind == KIND_PLUS ? SQRT2_D : -SQRT2_D) * (double)v.y, pi);
+    }
+}
+
+// Scatter a tile held in shared memory: element e (= smem index) maps to the
+// spectrum position coord(e) -> (ok, i, j, k).  U elements per thread are
+// decoded and their epilogue operands loaded before any is consumed.
+template <typename T, int U, class Epi, class Coord>
+__device__ __forceinline__ void scatter_tile(const cplx_t<T>* res, int total, const Geom& g, Coord coord, Epi& ep) {
+    for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
+        MapEntry en[U];
+        typename Epi::Pre pr[U], pi[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * blockDim.x;
+            int i = 0, j = 0, k = 0;
+            ok[u] = (e < total) && coord(e, i, j, k);
+            if (ok[u]) {
+                en[u] = decode(g, i, j, k);
+                ok[u] = en[u].src != 0;
+            }
+            if (ok[u]) {
+                pr[u] = ep.pre(en[u].re);
+                if (en[u].kind != KIND_VERT) pi[u] = ep.pre(en[u].im);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            const cplx_t<T> v = res[e0 + u * blockDim.x];
+            if (en[u].kind == KIND_VERT) {
+                ep.put(en[u].re, (double)v.x, pr[u]);
+            } else {
+                ep.put(en[u].re, SQRT2_D * (double)v.x, pr[u]);
+                ep.put(en[u].im, (en[u].kind == KIND_PLUS ? SQRT2_D : -SQRT2_D) * (double)v.y, pi[u]);
+            }
+        }
     }
 }
 
@@ -113,55 +197,98 @@ __device__ __forceinline__ void jk_of(int mode, int o, int x, int& j, int& k) {
     else { j = x; k = 0; }
 }
 
+constexpr int SCATTER_UNROLL = 4;
+
 // ------------------------------------------------------------ strided pass
+// Persistent: each CTA walks tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// A tile is TB consecutive dim-1 positions x one full line along the axis.
+// Shared memory: two load buffers (the next tile streams in by cp.async while
+// the current one is transformed) and one work buffer for the ping-pong stages.
 template <typename T, int TB, bool INV, int IN, int OUT, typename TS, class Epi>
-__global__ void __launch_bounds__(512) strided_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+__global__ void __launch_bounds__(256) strided_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* buf = reinterpret_cast<C*>(smem_raw);
     const int L = a.pl.L;
+    const int Lb = L * TB;
+    C* buf0 = reinterpret_cast<C*>(smem_raw);
+    C* buf1 = buf0 + Lb;
+    C* work = buf1 + Lb;
     __shared__ int s_rad[FFT_MAX_STAGES];
     load_radices(a.pl, s_rad);
-    C* alt = buf + (size_t)L * TB;
     const C* tw = a.tw;
     if (a.tw_in_smem) {
-        C* tws = buf + (size_t)2 * L * TB;
+        C* tws = work + Lb;
         for (int e = threadIdx.x; e < a.Ltab; e += blockDim.x) tws[e] = a.tw[e];
         tw = tws;
     }
-    const int i0 = blockIdx.x * TB;
-    const int o = blockIdx.y;
-    const int nb = min(TB, a.n_lines - i0);
-    const long long base = i0 + (long long)o * a.so;
-    for (int e = threadIdx.x; e < L * TB; e += blockDim.x) {
-        const int x = e / TB, b = e % TB;
-        C val = mk((T)0, (T)0);
-        if (b < nb) {
-            if (IN == IN_SPEC) {
-                val = a.spec[base + b + (long long)x * a.sx];
+    const int tiles_x = (a.n_lines + TB - 1) / TB;
+    const int ntiles = tiles_x * a.n_outer;
+    const C zero = mk((T)0, (T)0);
+
+    auto issue = [&](int t, C* dst) {
+        const int tx = t % tiles_x, o = t / tiles_x;
+        const int i0 = tx * TB, nb = min(TB, a.n_lines - i0);
+        const long long base = i0 + (long long)o * a.so;
+        for (int e = threadIdx.x; e < Lb; e += blockDim.x) {
+            const int x = e / TB, b = e % TB;
+            if (b < nb) {
+                if (IN == IN_SPEC) {
+                    cp_async<sizeof(C)>(&dst[e], a.spec + base + b + (long long)x * a.sx);
+                } else {
+                    int j, k;
+                    jk_of(a.jk_mode, o, x, j, k);
+                    gather_issue<T>(decode(a.g, i0 + b, j, k), src, &dst[e]);
+                }
             } else {
-                int j, k;
-                jk_of(a.jk_mode, o, x, j, k);
-                val = gather_val<T>(decode(a.g, i0 + b, j, k), src);
+                dst[e] = zero;
             }
         }
-        buf[e] = val;
-    }
-    __syncthreads();
-    const C* res = fft_lines<T, INV, true>(buf, alt, s_rad, a.pl.nst, L, TB, TB, tw, a.Ltab);
+    };
+
     Epi ep = epi;
-    for (int e = threadIdx.x; e < L * TB; e += blockDim.x) {
-        const int x = e / TB, b = e % TB;
-        if (b < nb) {
-            if (OUT == OUT_SPEC) {
-                a.spec[base + b + (long long)x * a.sx] = res[e];
-            } else {
-                int j, k;
-                jk_of(a.jk_mode, o, x, j, k);
-                scatter_val<T>(decode(a.g, i0 + b, j, k), res[e], ep);
+    int t = blockIdx.x;
+    if (t < ntiles) issue(t, buf0);
+    cp_async_commit();
+    for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+        C* cur = (it & 1) ? buf1 : buf0;
+        C* nxt = (it & 1) ? buf0 : buf1;
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, nxt);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const int tx = t % tiles_x, o = t / tiles_x;
+        const int i0 = tx * TB, nb = min(TB, a.n_lines - i0);
+        if (IN == IN_GATHER) {
+            for (int e = threadIdx.x; e < Lb; e += blockDim.x) {
+                const int x = e / TB, b = e % TB;
+                if (b < nb) {
+                    int j, k;
+                    jk_of(a.jk_mode, o, x, j, k);
+                    cur[e] = gather_combine<T>(decode(a.g, i0 + b, j, k), cur[e]);
+                }
             }
+            __syncthreads();
         }
+        const C* res = fft_lines<T, INV, true>(cur, work, s_rad, a.pl.nst, L, TB, TB, tw, a.Ltab);
+        if (OUT == OUT_SPEC) {
+            const long long base = i0 + (long long)o * a.so;
+            for (int e = threadIdx.x; e < Lb; e += blockDim.x) {
+                const int x = e / TB, b = e % TB;
+                if (b < nb) a.spec[base + b + (long long)x * a.sx] = res[e];
+            }
+        } else {
+            const int mode = a.jk_mode;
+            auto coord = [&](int e, int& i, int& j, int& k) -> bool {
+                const int x = e / TB, b = e % TB;
+                if (b >= nb) return false;
+                i = i0 + b;
+                jk_of(mode, o, x, j, k);
+                return true;
+            };
+            scatter_tile<T, SCATTER_UNROLL>(res, Lb, a.g, coord, ep);
+        }
+        __syncthreads();
     }
     if (OUT == OUT_SCATTER) ep.finish();
 }
@@ -180,8 +307,145 @@ __device__ __forceinline__ C r2c_post(C za, C zb, C w) {
     return csub(s, cmul_i(cmul(d, w)));
 }
 
-template <typename T, int IN, int OUT, bool MASK, bool PP, typename TS, class Epi>
-__global__ void __launch_bounds__(PP ? 512 : 1024) row_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+// Persistent double-buffered row pass: tiles of RB rows along dim 1
+// (rows = (j, k) pairs), each row M+1 half-spectrum values, interleaved in
+// shared memory as buf[n*TBP + b].
+template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
+__global__ void __launch_bounds__(256) row_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    using C = cplx_t<T>;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int M = a.g.m1;
+    const int RB = a.rb, TBP = a.tbp;
+    const size_t span = (size_t)(M + 1) * TBP;
+    C* buf0 = reinterpret_cast<C*>(smem_raw);
+    C* buf1 = buf0 + span;
+    C* work = buf1 + span;
+    __shared__ int s_rad[FFT_MAX_STAGES];
+    load_radices(a.pl, s_rad);
+    const C* tw = a.tw;
+    if (a.tw_in_smem) {
+        C* tws = work + span;
+        for (int e = threadIdx.x; e < a.Ltab; e += blockDim.x) tws[e] = a.tw[e];
+        tw = tws;
+    }
+    const int ntiles = (a.nrows + RB - 1) / RB;
+    const C zero = mk((T)0, (T)0);
+    const int half = M / 2;
+
+    auto issue = [&](int t, C* dst) {
+        const int r0 = t * RB, nr = min(RB, a.nrows - r0);
+        if (IN == IN_REAL) {
+            for (int e = threadIdx.x; e < M * RB; e += blockDim.x) {
+                const int b = e / M, n = e % M;
+                if (b < nr) cp_async<sizeof(C)>(&dst[n * TBP + b], a.real_in + (size_t)(r0 + b) * a.g.n1 + 2 * n);
+                else dst[n * TBP + b] = zero;
+            }
+        } else {
+            for (int e = threadIdx.x; e < (M + 1) * RB; e += blockDim.x) {
+                const int b = e / (M + 1), n = e % (M + 1);
+                if (b < nr) {
+                    if (IN == IN_SPEC) cp_async<sizeof(C)>(&dst[n * TBP + b], a.spec + (size_t)(r0 + b) * a.g.ld1 + n);
+                    else gather_issue<T>(decode1(a.g, n), src, &dst[n * TBP + b]);
+                } else {
+                    dst[n * TBP + b] = zero;
+                }
+            }
+        }
+    };
+
+    Epi ep = epi;
+    int t = blockIdx.x;
+    if (t < ntiles) issue(t, buf0);
+    cp_async_commit();
+    for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+        C* cur = (it & 1) ? buf1 : buf0;
+        C* nxt = (it & 1) ? buf0 : buf1;
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, nxt);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const int r0 = t * RB, nr = min(RB, a.nrows - r0);
+        if (IN == IN_GATHER) {
+            for (int n = threadIdx.x; n <= M; n += blockDim.x) cur[n * TBP] = gather_combine<T>(decode1(a.g, n), cur[n * TBP]);
+            __syncthreads();
+        }
+        C* c1 = cur;
+        if (IN != IN_REAL) {
+            for (int e = threadIdx.x; e < (half + 1) * RB; e += blockDim.x) {
+                const int b = e % RB, k = e / RB;
+                if (k == 0) {
+                    const C x0 = cur[b], xm = cur[M * TBP + b];
+                    cur[b] = c2r_pre(x0, xm, tw[0]);
+                } else if (2 * k == M) {
+                    const C xk = cur[k * TBP + b];
+                    cur[k * TBP + b] = c2r_pre(xk, xk, tw[k]);
+                } else {
+                    const C xk = cur[k * TBP + b], xm = cur[(M - k) * TBP + b];
+                    cur[k * TBP + b] = c2r_pre(xk, xm, tw[k]);
+                    cur[(M - k) * TBP + b] = c2r_pre(xm, xk, tw[M - k]);
+                }
+            }
+            __syncthreads();
+            c1 = fft_lines<T, true, true>(cur, work, s_rad, a.pl.nst, M, RB, TBP, tw, a.Ltab);
+        }
+        // scale and mask the real samples (x[2n], x[2n+1]) = (Re z[n], Im z[n])
+        const T sc = (T)a.scale;
+        for (int e = threadIdx.x; e < M * RB; e += blockDim.x) {
+            const int b = e / M, n = e % M;
+            if (b < nr) {
+                C y = c1[n * TBP + b];
+                y.x *= sc;
+                y.y *= sc;
+                if (MASK) {
+                    const uint32_t w = a.maskw[(size_t)(r0 + b) * a.wpr + (n >> 4)];
+                    const int sh = (2 * n) & 31;
+                    if (!((w >> sh) & 1u)) y.x = (T)0;
+                    if (!((w >> (sh + 1)) & 1u)) y.y = (T)0;
+                }
+                if (OUT == OUT_REAL) *reinterpret_cast<C*>(a.real_out + (size_t)(r0 + b) * a.g.n1 + 2 * n) = y;
+                else c1[n * TBP + b] = y;
+            }
+        }
+        if (OUT != OUT_REAL) {
+            __syncthreads();
+            C* other = (c1 == cur) ? work : cur;
+            C* c2 = fft_lines<T, false, true>(c1, other, s_rad, a.pl.nst, M, RB, TBP, tw, a.Ltab);
+            for (int e = threadIdx.x; e < (half + 1) * RB; e += blockDim.x) {
+                const int b = e % RB, k = e / RB;
+                if (k == 0) {
+                    const C z0 = c2[b];
+                    c2[b] = r2c_post(z0, z0, tw[0]);
+                    c2[M * TBP + b] = mk((T)2 * (z0.x - z0.y), (T)0);
+                } else if (2 * k == M) {
+                    const C zk = c2[k * TBP + b];
+                    c2[k * TBP + b] = r2c_post(zk, zk, tw[k]);
+                } else {
+                    const C zk = c2[k * TBP + b], zm = c2[(M - k) * TBP + b];
+                    c2[k * TBP + b] = r2c_post(zk, zm, tw[k]);
+                    c2[(M - k) * TBP + b] = r2c_post(zm, zk, tw[M - k]);
+                }
+            }
+            __syncthreads();
+            if (OUT == OUT_SPEC) {
+                for (int e = threadIdx.x; e < (M + 1) * RB; e += blockDim.x) {
+                    const int b = e / (M + 1), n = e % (M + 1);
+                    if (b < nr) a.spec[(size_t)(r0 + b) * a.g.ld1 + n] = c2[n * TBP + b];
+                }
+            } else {   // 1D: one row, TBP == 1
+                auto coord = [&](int e, int& i, int& j, int& k) -> bool { i = e; j = 0; k = 0; return true; };
+                scatter_tile<T, SCATTER_UNROLL>(c2, M + 1, a.g, coord, ep);
+            }
+        }
+        __syncthreads();
+    }
+    if (OUT == OUT_SCATTER) ep.finish();
+}
+
+// In-place row pass for rows too long to double-buffer (1D with large N):
+// single tile, register-staged stages.
+template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
+__global__ void __launch_bounds__(1024) row_pass_ip_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -190,8 +454,9 @@ __global__ void __launch_bounds__(PP ? 512 : 1024) row_pass_kernel(PassArgs<T> a
     const int RB = a.rb, TBP = a.tbp;
     __shared__ int s_rad[FFT_MAX_STAGES];
     load_radices(a.pl, s_rad);
+    constexpr bool PP = false;
     const size_t span = (size_t)(M + 1) * TBP;
-    C* alt = PP ? buf + span : nullptr;
+    C* alt = nullptr;
     const C* tw = a.tw;
     if (a.tw_in_smem) {
         C* tws = buf + (PP ? 2 : 1) * span;
@@ -288,7 +553,7 @@ __global__ void __launch_bounds__(PP ? 512 : 1024) row_pass_kernel(PassArgs<T> a
         }
     } else {
         Epi ep = epi;
-        for (int n = threadIdx.x; n <= M; n += blockDim.x) scatter_val<T>(decode1(a.g, n), buf[n * TBP], ep);
+        for (int n = threadIdx.x; n <= M; n += blockDim.x) scatter_one<T>(decode1(a.g, n), buf[n * TBP], ep);
         ep.finish();
     }
 }
@@ -300,8 +565,9 @@ struct PassCfg {
     int threads = 0;
     size_t smem = 0;
     int tw_in_smem = 0;
-    int pp = 1;          // 1: double-buffered (ping-pong) stages, 0: in place
-    dim3 grid;
+    int pp = 1;          // 1: persistent, double-buffered loads + ping-pong stages; 0: in place, one tile
+    int tiles = 0;       // number of tiles of the pass
+    dim3 grid;           // in-place path only; persistent grids are sized from occupancy at launch
 };
 
 template <typename T>
@@ -345,64 +611,70 @@ public:
     // conservative dynamic shared-memory budget per CTA (B200 opt-in limit is 227 KB incl. static)
     static size_t smem_limit() { return 200 * 1024; }
 
-    // Strided passes always double-buffer: TB lines of L elements, twice.
+    // Strided passes: three shared buffers of TB lines (two load stages + one
+    // work buffer), TB a power of two chosen so a CTA takes ~64 KB.
     bool choose_strided(const FftPlanDev& pl, int Ltab, int n_lines, int n_outer, PassCfg* cfg, std::string* err) {
         const int L = pl.L;
-        const int cands[4] = {sizeof(T) == 8 ? 8 : 16, sizeof(T) == 8 ? 4 : 8, sizeof(T) == 8 ? 2 : 4, 2};
-        for (int tb : cands) {
-            const size_t data = 2 * (size_t)L * tb * sizeof(C);
-            if (data > smem_limit()) continue;
-            int thr = ((L * tb) / 4 + 31) / 32 * 32;
-            thr = std::max(64, std::min(512, thr));
-            cfg->tb = tb;
-            cfg->tbp = tb;
-            cfg->threads = thr;
-            cfg->pp = 1;
-            const size_t tws = (size_t)Ltab * sizeof(C);
-            cfg->tw_in_smem = (data + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
-            cfg->smem = data + (cfg->tw_in_smem ? tws : 0);
-            cfg->grid = dim3((n_lines + tb - 1) / tb, n_outer, 1);
-            return true;
+        const size_t per_line = (size_t)L * sizeof(C);
+        int tb = 16;
+        while (tb > 2 && 3 * per_line * tb > 64 * 1024) tb /= 2;
+        if (sizeof(T) == 8 && tb > 8) tb = 8;
+        const size_t data = 3 * per_line * tb;
+        if (data > smem_limit()) {
+            *err = "transform length too large for the on-chip strided pass";
+            return false;
         }
-        *err = "transform length too large for the on-chip strided pass";
-        return false;
+        cfg->tb = tb;
+        cfg->tbp = tb;
+        cfg->threads = 256;
+        cfg->pp = 1;
+        const size_t tws = (size_t)Ltab * sizeof(C);
+        cfg->tw_in_smem = (data + tws <= smem_limit() && tws <= 32 * 1024) ? 1 : 0;
+        cfg->smem = data + (cfg->tw_in_smem ? tws : 0);
+        cfg->tiles = ((n_lines + tb - 1) / tb) * n_outer;
+        cfg->grid = dim3(cfg->tiles, 1, 1);
+        return true;
     }
 
-    // Row passes double-buffer when two copies fit in shared memory, else they
-    // run in place with the register-staged stages.
+    // Row passes: persistent with three buffers when they fit, else one
+    // in-place tile per CTA (very long rows, 1D).
     bool choose_row(int nrows, PassCfg* cfg, std::string* err) {
         const int M = g.m1;
         const int Ltab = g.n1;
         const size_t tws = (size_t)Ltab * sizeof(C);
         int rb = 1;
-        while (rb < 16 && rb * 2 <= nrows && (size_t)(M + 1) * (rb * 2 + 1) * sizeof(C) <= 24 * 1024) rb *= 2;
-        for (; rb >= 1; rb /= 2) {
-            const int tbp = rb > 1 ? rb + 1 : 1;
-            const size_t one = (size_t)(M + 1) * tbp * sizeof(C);
-            if (2 * one <= smem_limit()) {
-                int thr = ((M * rb) / 4 + 31) / 32 * 32;
-                thr = std::max(64, std::min(512, thr));
-                cfg->pp = 1;
-                cfg->tb = rb;
-                cfg->tbp = tbp;
-                cfg->threads = thr;
-                cfg->tw_in_smem = (2 * one + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
-                cfg->smem = 2 * one + (cfg->tw_in_smem ? tws : 0);
-                cfg->grid = dim3((nrows + rb - 1) / rb, 1, 1);
-                return true;
-            }
-            if (one > smem_limit()) continue;
+        while (rb < 16 && rb * 2 <= nrows && 3 * (size_t)(M + 1) * (rb * 2 + 1) * sizeof(C) <= 72 * 1024) rb *= 2;
+        const int tbp = rb > 1 ? rb + 1 : 1;
+        const size_t one = (size_t)(M + 1) * tbp * sizeof(C);
+        if (3 * one <= smem_limit()) {
+            cfg->pp = 1;
+            cfg->tb = rb;
+            cfg->tbp = tbp;
+            cfg->threads = 256;
+            cfg->tw_in_smem = (3 * one + tws <= smem_limit() && tws <= 32 * 1024) ? 1 : 0;
+            cfg->smem = 3 * one + (cfg->tw_in_smem ? tws : 0);
+            cfg->tiles = (nrows + rb - 1) / rb;
+            cfg->grid = dim3(cfg->tiles, 1, 1);
+            return true;
+        }
+        // in place: the register-staged engine takes radices <= 8
+        if (!make_fft_plan(M, &plan1, err, 8)) return false;
+        for (rb = 1; rb >= 1; rb /= 2) {
+            const int tp = 1;
+            const size_t o1 = (size_t)(M + 1) * tp * sizeof(C);
+            if (o1 > smem_limit()) break;
             int thr = ((M * rb + 7) / 8 + 31) / 32 * 32;
             thr = std::max(64, std::min(1024, thr));
             while (thr < 1024 && !plan_fits(plan1, rb, thr)) thr += 32;
-            if (!plan_fits(plan1, rb, thr)) continue;
+            if (!plan_fits(plan1, rb, thr)) break;
             cfg->pp = 0;
             cfg->tb = rb;
-            cfg->tbp = tbp;
+            cfg->tbp = tp;
             cfg->threads = thr;
-            cfg->tw_in_smem = (one + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
-            cfg->smem = one + (cfg->tw_in_smem ? tws : 0);
-            cfg->grid = dim3((nrows + rb - 1) / rb, 1, 1);
+            cfg->tw_in_smem = (o1 + tws <= smem_limit() && tws <= 64 * 1024) ? 1 : 0;
+            cfg->smem = o1 + (cfg->tw_in_smem ? tws : 0);
+            cfg->tiles = (nrows + rb - 1) / rb;
+            cfg->grid = dim3(cfg->tiles, 1, 1);
             return true;
         }
         *err = "dimension 1 too large for the on-chip row pass";
@@ -410,12 +682,21 @@ public:
     }
 
     // host_keep: N bytes (1 = observed) or nullptr for no mask
+    // largest register radix of the double-buffered stages (FP64 keeps 20
+    // complex values per thread, FP32 32)
+    static int max_radix() { return 8; }
+
+    bool make_plans(std::string* err) {
+        if (!make_fft_plan(g.m1, &plan1, err, max_radix())) return false;
+        if (g.dim >= 2 && !make_fft_plan(g.n2, &plan2, err, max_radix())) return false;
+        if (g.dim >= 3 && !make_fft_plan(g.n3, &plan3, err, max_radix())) return false;
+        return true;
+    }
+
     bool init(const Geom& geom, const uint8_t* host_keep, cudaStream_t st, std::string* err) {
         g = geom;
         stream = st;
-        if (!make_fft_plan(g.m1, &plan1, err)) return false;
-        if (g.dim >= 2 && !make_fft_plan(g.n2, &plan2, err)) return false;
-        if (g.dim >= 3 && !make_fft_plan(g.n3, &plan3, err)) return false;
+        if (!make_plans(err)) return false;
         const int nrows = g.n2 * g.n3;
         if (!choose_row(nrows, &row_cfg, err)) return false;
         if (g.dim >= 2 && !choose_strided(plan2, g.n2, g.m1 + 1, g.dim == 3 ? g.n3 : 1, &s2_cfg, err)) return false;
@@ -454,10 +735,10 @@ public:
         a.n_lines = g.m1 + 1;
         if (axis == 3) {
             a.pl = plan3; a.tw = tw3; a.Ltab = g.n3; a.tw_in_smem = s3_cfg.tw_in_smem;
-            a.so = g.ld1; a.sx = (long long)g.ld1 * g.n2; a.jk_mode = 0;
+            a.so = g.ld1; a.sx = (long long)g.ld1 * g.n2; a.jk_mode = 0; a.n_outer = g.n2;
         } else {
             a.pl = plan2; a.tw = tw2; a.Ltab = g.n2; a.tw_in_smem = s2_cfg.tw_in_smem;
-            a.so = (long long)g.ld1 * g.n2; a.sx = g.ld1; a.jk_mode = g.dim == 3 ? 1 : 2;
+            a.so = (long long)g.ld1 * g.n2; a.sx = g.ld1; a.jk_mode = g.dim == 3 ? 1 : 2; a.n_outer = g.dim == 3 ? g.n3 : 1;
         }
         return a;
     }
@@ -491,6 +772,30 @@ inline cudaError_t smem_optin(K kernel, size_t smem) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
 }
 
+// Persistent grid: resident CTAs per SM (occupancy API, cached per kernel,
+// device and configuration) times the SM count, capped by the tile count.
+inline int persistent_grid(const void* fn, int threads, size_t smem, int tiles) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(fn, dev, threads, smem);
+    int per_sm = 0, sms = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) per_sm = it->second;
+    }
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = per_sm;
+    }
+    const long long g = (long long)per_sm * (sms > 0 ? sms : 148);
+    return (int)std::max<long long>(1, std::min<long long>(g, tiles));
+}
+
 // Launch helpers (template dispatch on TB).
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
 inline cudaError_t launch_strided(const PassCfg& c, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
@@ -501,7 +806,8 @@ inline cudaError_t launch_strided(const PassCfg& c, const PassArgs<T>& a, const 
             auto k = strided_pass_kernel<T, TBV, INV, IN, OUT, TS, Epi>;                              \
             e = smem_optin(k, c.smem);                                                                \
             if (e != cudaSuccess) return e;                                                           \
-            k<<<c.grid, c.threads, c.smem, st>>>(a, src, epi);                                        \
+            const int grid = persistent_grid((const void*)k, c.threads, c.smem, c.tiles);             \
+            k<<<grid, c.threads, c.smem, st>>>(a, src, epi);                                          \
         } break;
         CSIPM_TB_CASE(2) CSIPM_TB_CASE(4) CSIPM_TB_CASE(8) CSIPM_TB_CASE(16)
 #undef CSIPM_TB_CASE
@@ -512,10 +818,18 @@ inline cudaError_t launch_strided(const PassCfg& c, const PassArgs<T>& a, const 
 
 template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
 inline cudaError_t launch_row(const PassCfg& c, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
-    auto k = c.pp ? row_pass_kernel<T, IN, OUT, MASK, true, TS, Epi> : row_pass_kernel<T, IN, OUT, MASK, false, TS, Epi>;
-    cudaError_t e = smem_optin(k, c.smem);
-    if (e != cudaSuccess) return e;
-    k<<<c.grid, c.threads, c.smem, st>>>(a, src, epi);
+    if (c.pp) {
+        auto k = row_pass_kernel<T, IN, OUT, MASK, TS, Epi>;
+        cudaError_t e = smem_optin(k, c.smem);
+        if (e != cudaSuccess) return e;
+        const int grid = persistent_grid((const void*)k, c.threads, c.smem, c.tiles);
+        k<<<grid, c.threads, c.smem, st>>>(a, src, epi);
+    } else {
+        auto k = row_pass_ip_kernel<T, IN, OUT, MASK, TS, Epi>;
+        cudaError_t e = smem_optin(k, c.smem);
+        if (e != cudaSuccess) return e;
+        k<<<c.grid, c.threads, c.smem, st>>>(a, src, epi);
+    }
     return cudaGetLastError();
 }
 

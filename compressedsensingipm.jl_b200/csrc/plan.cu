@@ -4,13 +4,35 @@
 
 namespace csipm {
 
-bool make_fft_plan(int L, FftPlanDev* out, std::string* err) {
+bool make_fft_plan(int L, FftPlanDev* out, std::string* err, int max_radix) {
     FftPlanDev p{};
     p.L = L;
     p.nst = 0;
     if (L < 1) {
         if (err) *err = "FFT length must be positive";
         return false;
+    }
+    if (max_radix > 8) {
+        static const int cand[] = {32, 25, 20, 16, 15, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+        int r = L;
+        while (r > 1) {
+            int pick = 0;
+            for (int c : cand)
+                if (c <= max_radix && r % c == 0) { pick = c; break; }
+            if (!pick) {   // a prime > 7 (or a composite of them): smallest factor as a direct DFT
+                pick = r;
+                for (int f = 11; (long long)f * f <= r; f += 2)
+                    if (r % f == 0) { pick = f; break; }
+            }
+            if (p.nst >= FFT_MAX_STAGES) {
+                if (err) *err = "FFT length has too many prime factors";
+                return false;
+            }
+            p.rad[p.nst++] = pick;
+            r /= pick;
+        }
+        *out = p;
+        return true;
     }
     int r = L;
     int twos = 0;

@@ -7,9 +7,13 @@
 
 namespace csipm {
 
-// Factor L into stages: radix 8 first, then 4/2 for the rest of the power of
-// two, then 5, 3, 7 and finally any other prime as a direct DFT stage.
-bool make_fft_plan(int L, FftPlanDev* out, std::string* err);
+// Factor L into stages.  max_radix <= 8: radix 8 first, then 4/2 for the rest
+// of the power of two, then 5, 3, 7 (the register-staged in-place engine).
+// Larger max_radix: greedy largest-first over the composite register radices
+// {32, 25, 20, 16, 15, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2} up to max_radix, which
+// cuts the number of shared-memory round trips (320 = 20*16, 160 = 20*8).
+// Any remaining prime becomes a direct-DFT stage.
+bool make_fft_plan(int L, FftPlanDev* out, std::string* err, int max_radix = 8);
 
 // exp(-2*pi*i*e/L) for e = 0..L-1, rounded from long double.
 void twiddle_table(int L, std::vector<double>* re_im);

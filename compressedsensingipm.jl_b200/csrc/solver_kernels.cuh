@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <float.h>
 
+#include "operator.cuh"
 #include "reduce.cuh"
 
 namespace csipm {
@@ -38,7 +39,7 @@ struct CgScalars {
 // r = rhs - q (q = (Q + D) x0 computed by the operator), or r = rhs when x0 == 0;
 // z = Minv r ; p = z ; rz = r.z ; thresh = atol + rtol*sqrt(rz)
 template <typename TV>
-__global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
+static __global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
                                const TV* __restrict__ Minv, TV* __restrict__ r, TV* __restrict__ p,
                                RedWorkspace ws, CgScalars* sc, double atol, double rtol) {
     double acc[1] = {0.0};
@@ -64,7 +65,7 @@ __global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, cons
 
 // alpha = rz/pq ; x += alpha p ; r -= alpha q ; rz' = r.(Minv r)
 template <typename TV, typename TX>
-__global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
+static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
                                  const TV* __restrict__ q, const TV* __restrict__ Minv, RedWorkspace ws, CgScalars* sc) {
     if (sc->done) return;
     const double pq = sc->pq;
@@ -89,7 +90,7 @@ __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __
 
 // p = Minv r + (rz'/rz) p
 template <typename TV>
-__global__ void cg_pupdate_kernel(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
+static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
                                   const CgScalars* sc) {
     if (sc->done) return;
     const double b = sc->rz[(it + 1) & 1] / sc->rz[it & 1];
@@ -105,7 +106,7 @@ enum { RR_SZ = 0, RR_BB, RR_BQB, RR_L1, RR_GINF, RR_RDINF, RR_RCINF, RR_SUMC, RR
 constexpr unsigned RR_MAXMASK = (1u << RR_GINF) | (1u << RR_RDINF) | (1u << RR_RCINF);
 
 // beta = soft(b, lambda); reduce max|beta| and max|b|
-__global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
+static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
                                  RedWorkspace ws) {
     double acc[2] = {0.0, 0.0};
     CSIPM_GRID_LOOP(i, n) {
@@ -122,7 +123,7 @@ __global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, doub
 // Dual start from the clipped gradient with lz = max(lambda, 1e-3 |b|_inf, 1e-12)
 // (the floor keeps lambda = 0 interior); c = |beta| + mu0/min(z1,z2),
 // mu0 = 0.1*lz*max(1e-3, max|beta|).  mx = {max|beta|, max|b|}.
-__global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                                  const double* __restrict__ beta, const double* __restrict__ mx,
                                  double* __restrict__ c, double* __restrict__ z1, double* __restrict__ z2) {
     const double lz = fmax(fmax(lam, 1e-3 * mx[1]), 1e-12);
@@ -138,7 +139,7 @@ __global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, cons
 }
 
 // rd = Qb - b - z1 + z2 (stored) and the scalar diagnostics
-__global__ void ipm_residual_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+static __global__ void ipm_residual_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                                     const double* __restrict__ beta, const double* __restrict__ c,
                                     const double* __restrict__ z1, const double* __restrict__ z2,
                                     double* __restrict__ rd, RedWorkspace ws) {
@@ -163,7 +164,7 @@ __global__ void ipm_residual_kernel(long long n, const double* __restrict__ b, c
 
 // Barrier diagonals of the condensed Schur system: Db = 4 D1 D2/(D1 + D2), Minv = 1/(1 + Db)
 template <typename TV>
-__global__ void ipm_diag_kernel(long long n, const double* __restrict__ beta, const double* __restrict__ c,
+static __global__ void ipm_diag_kernel(long long n, const double* __restrict__ beta, const double* __restrict__ c,
                                 const double* __restrict__ z1, const double* __restrict__ z2,
                                 double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
                                 TV* __restrict__ Minv_lo, int precond) {
@@ -201,7 +202,7 @@ __device__ __forceinline__ ElemDir elem_direction(double be, double ce, double a
 }
 
 // rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 ; corrector uses the affine direction dba
-__global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
                                const double* __restrict__ z1, const double* __restrict__ z2,
                                const double* __restrict__ rd, const double* __restrict__ dba, double sigmu,
                                double* __restrict__ rhs) {
@@ -228,7 +229,7 @@ __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict
 enum { SS_MINP = 0, SS_MIND, SS_SZ, SS_CROSS, SS_DD, SS_N };
 constexpr unsigned SS_MINMASK = (1u << SS_MINP) | (1u << SS_MIND);
 
-__global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
                                      const double* __restrict__ z1, const double* __restrict__ z2,
                                      const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
                                      RedWorkspace ws) {
@@ -255,7 +256,7 @@ __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __re
 }
 
 // beta += ap db ; c += ap dc ; z += ad dz
-__global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ c,
+static __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ c,
                                   double* __restrict__ z1, double* __restrict__ z2, const double* __restrict__ dba,
                                   double sigmu, const double* __restrict__ db, double ap, double ad) {
     CSIPM_GRID_LOOP(i, n) {
@@ -277,21 +278,21 @@ __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ 
 
 // ------------------------------------------------------------------ utilities
 template <typename TA, typename TB>
-__global__ void convert_kernel(long long n, const TA* __restrict__ a, TB* __restrict__ b) {
+static __global__ void convert_kernel(long long n, const TA* __restrict__ a, TB* __restrict__ b) {
     CSIPM_GRID_LOOP(i, n) b[i] = (TB)a[i];
 }
 
-__global__ void axpy_kernel(long long n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
+static __global__ void axpy_kernel(long long n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
     CSIPM_GRID_LOOP(i, n) y[i] += alpha * x[i];
 }
 
 // y = x - y  (residual r = rhs - Kx in place on y)
-__global__ void sub_from_kernel(long long n, const double* __restrict__ x, double* __restrict__ y) {
+static __global__ void sub_from_kernel(long long n, const double* __restrict__ x, double* __restrict__ y) {
     CSIPM_GRID_LOOP(i, n) y[i] = x[i] - y[i];
 }
 
 // dot products on the device
-__global__ void dot2_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+static __global__ void dot2_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
                             const double* __restrict__ c2, const double* __restrict__ d2, RedWorkspace ws) {
     double acc[2] = {0.0, 0.0};
     CSIPM_GRID_LOOP(i, n) {
@@ -306,16 +307,18 @@ __global__ void dot2_kernel(long long n, const double* __restrict__ a, const dou
 struct EpiGrad {
     const double* b;
     double* g;
-    __device__ __forceinline__ void put(int l, double v) { g[l] = v - b[l]; }
+    using Pre = NoPre;
+    __device__ __forceinline__ NoPre pre(int) const { return {}; }
+    __device__ __forceinline__ void put(int l, double v, const NoPre&) { g[l] = v - b[l]; }
     __device__ __forceinline__ void finish() {}
 };
 
-__global__ void fill_kernel(long long n, double v, double* __restrict__ y) {
+static __global__ void fill_kernel(long long n, double v, double* __restrict__ y) {
     CSIPM_GRID_LOOP(i, n) y[i] = v;
 }
 
 // cons!: c = [-beta - c ; beta - c]   (src/fft_model.jl:91-101)
-__global__ void cons_kernel(long long n, const double* __restrict__ x, double* __restrict__ out) {
+static __global__ void cons_kernel(long long n, const double* __restrict__ x, double* __restrict__ out) {
     CSIPM_GRID_LOOP(i, n) {
         const double be = x[i], ce = x[n + i];
         out[i] = -be - ce;
@@ -327,12 +330,14 @@ __global__ void cons_kernel(long long n, const double* __restrict__ x, double* _
 struct EpiScale {
     double w;
     double* out;
-    __device__ __forceinline__ void put(int l, double v) { out[l] = w * v; }
+    using Pre = NoPre;
+    __device__ __forceinline__ NoPre pre(int) const { return {}; }
+    __device__ __forceinline__ void put(int l, double v, const NoPre&) { out[l] = w * v; }
     __device__ __forceinline__ void finish() {}
 };
 
 // build_kkt!  (src/fft_kkt.jl:285-307)
-__global__ void kkt_build_kernel(long long n, const double* __restrict__ pr_diag, double* __restrict__ L1,
+static __global__ void kkt_build_kernel(long long n, const double* __restrict__ pr_diag, double* __restrict__ L1,
                                  double* __restrict__ L2, double* __restrict__ P11, double* __restrict__ P12,
                                  double* __restrict__ P22) {
     CSIPM_GRID_LOOP(i, n) {
@@ -357,7 +362,9 @@ struct EpiCondensed {
     const double* L2;
     long long n;
     double alpha, beta;
-    __device__ __forceinline__ void put(int l, double v) {
+    using Pre = NoPre;
+    __device__ __forceinline__ NoPre pre(int) const { return {}; }
+    __device__ __forceinline__ void put(int l, double v, const NoPre&) {
         const double xb = x[l], xz = x[n + l];
         const double l1 = L1[l], l2 = L2[l];
         y[l] = beta * y[l] + alpha * (v + l1 * xb + l2 * xz);
@@ -367,7 +374,7 @@ struct EpiCondensed {
 };
 
 // preconditioner mul!  (src/fft_kkt.jl:73-85)
-__global__ void precond_mul_kernel(long long n, double* __restrict__ y, const double* __restrict__ x,
+static __global__ void precond_mul_kernel(long long n, double* __restrict__ y, const double* __restrict__ x,
                                    const double* __restrict__ P11, const double* __restrict__ P12,
                                    const double* __restrict__ P22, double alpha, double beta) {
     CSIPM_GRID_LOOP(i, n) {
@@ -383,7 +390,9 @@ struct EpiKKT {
     double* y;          // 6N
     long long n;
     double alpha, beta;
-    __device__ __forceinline__ void put(int l, double v) {
+    using Pre = NoPre;
+    __device__ __forceinline__ NoPre pre(int) const { return {}; }
+    __device__ __forceinline__ void put(int l, double v, const NoPre&) {
         const long long N = n;
         const double xb = x[l], xz = x[N + l], xs1 = x[2 * N + l], xs2 = x[3 * N + l];
         const double xy1 = x[4 * N + l], xy2 = x[5 * N + l];
@@ -398,7 +407,7 @@ struct EpiKKT {
 };
 
 // jtprod!  (src/fft_kkt.jl:253-275)
-__global__ void jtprod_kernel(long long n, double* __restrict__ y, const double* __restrict__ x) {
+static __global__ void jtprod_kernel(long long n, double* __restrict__ y, const double* __restrict__ x) {
     CSIPM_GRID_LOOP(i, n) {
         const double y1 = x[i], y2 = x[n + i];
         y[i] = -y1 + y2;
@@ -409,7 +418,7 @@ __global__ void jtprod_kernel(long long n, double* __restrict__ y, const double*
 }
 
 // solve_kkt! right-hand side (src/fft_kkt.jl:334-335): b = [w1 - w3 + w4 - S1 w5 + S2 w6 ; w2 - w3 - w4 - S1 w5 - S2 w6]
-__global__ void kkt_rhs_kernel(long long n, const double* __restrict__ w, const double* __restrict__ pr_diag,
+static __global__ void kkt_rhs_kernel(long long n, const double* __restrict__ w, const double* __restrict__ pr_diag,
                                double* __restrict__ b) {
     CSIPM_GRID_LOOP(i, n) {
         const double S1 = pr_diag[2 * n + i], S2 = pr_diag[3 * n + i];
@@ -420,7 +429,7 @@ __global__ void kkt_rhs_kernel(long long n, const double* __restrict__ w, const 
 }
 
 // solve_kkt! back-substitution (src/fft_kkt.jl:345-350)
-__global__ void kkt_back_kernel(long long n, double* __restrict__ w, const double* __restrict__ x,
+static __global__ void kkt_back_kernel(long long n, double* __restrict__ w, const double* __restrict__ x,
                                 const double* __restrict__ pr_diag) {
     CSIPM_GRID_LOOP(i, n) {
         const double S1 = pr_diag[2 * n + i], S2 = pr_diag[3 * n + i];
@@ -448,7 +457,7 @@ __device__ __forceinline__ void pblock(const double* P11, const double* P12, con
 }
 
 // x = 0, r = b, p = z = P r, rz = r.z
-__global__ void kcg_init_kernel(long long n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
+static __global__ void kcg_init_kernel(long long n, const double* __restrict__ b, double* __restrict__ x, double* __restrict__ r,
                                 double* __restrict__ p, const double* __restrict__ P11, const double* __restrict__ P12,
                                 const double* __restrict__ P22, RedWorkspace ws, CgScalars* sc, double atol, double rtol) {
     double acc[1] = {0.0};
@@ -481,9 +490,11 @@ struct EpiKcg {
     long long n;
     RedWorkspace ws;
     double acc;
-    __device__ __forceinline__ void put(int l, double v) {
-        const double pb = p[l], pz = p[n + l];
-        const double l1 = L1[l], l2 = L2[l];
+    struct Pre { double pb, pz, l1, l2; };
+    __device__ __forceinline__ Pre pre(int l) const { return Pre{p[l], p[n + l], L1[l], L2[l]}; }
+    __device__ __forceinline__ void put(int l, double v, const Pre& r) {
+        const double pb = r.pb, pz = r.pz;
+        const double l1 = r.l1, l2 = r.l2;
         const double qb = v + l1 * pb + l2 * pz;
         const double qz = l2 * pb + l1 * pz;
         q[l] = qb;
@@ -496,7 +507,7 @@ struct EpiKcg {
     }
 };
 
-__global__ void kcg_update_kernel(long long n, int it, double* __restrict__ x, double* __restrict__ r,
+static __global__ void kcg_update_kernel(long long n, int it, double* __restrict__ x, double* __restrict__ r,
                                   const double* __restrict__ p, const double* __restrict__ q,
                                   const double* __restrict__ P11, const double* __restrict__ P12,
                                   const double* __restrict__ P22, RedWorkspace ws, CgScalars* sc) {
@@ -524,7 +535,7 @@ __global__ void kcg_update_kernel(long long n, int it, double* __restrict__ x, d
     }
 }
 
-__global__ void kcg_pupdate_kernel(long long n, int it, const double* __restrict__ r, double* __restrict__ p,
+static __global__ void kcg_pupdate_kernel(long long n, int it, const double* __restrict__ r, double* __restrict__ p,
                                    const double* __restrict__ P11, const double* __restrict__ P12,
                                    const double* __restrict__ P22, const CgScalars* sc) {
     if (sc->done) return;

@@ -13,7 +13,7 @@ CPU FP64 restatement of the solver layer:
   condensed Newton system of src/fft_kkt.jl with dc eliminated (Schur
   complement A'A + Db, preconditioner 1/(1+Db)), fraction-to-boundary
   max(0.99, 1-mu), stop on the relative LASSO duality gap or on the scaled
-  KKT error max(|rd|, |rc|, mu)/max(1, |A'z0|_inf).  MadNLP itself is
+  KKT error max(max(|rd|, |rc|)/max(1, |A'z0|_inf), s'z/max(1, |F|)).  MadNLP itself is
   external to the reference and absent here, so this is the CPU twin of the
   GPU algorithm, not a restatement of MadNLP; iteration-count parity with
   MadNLP is unpinned.
@@ -231,7 +231,7 @@ def ipm(op, b, lam, z0sq, tol=1e-8, max_iter=2000, cg_rtol=1e-8, cg_maxit=None, 
         gap = (F - D) / max(abs(F), 1e-300)
         # scaled KKT error (dual infeasibility, complementarity), the criterion that
         # still applies when lambda = 0 makes the LASSO dual bound degenerate
-        kkt = max(np.abs(rd).max(), np.abs(rc).max(), mu) / max(1.0, binf)
+        kkt = max(max(np.abs(rd).max(), np.abs(rc).max()) / max(1.0, binf), (s1 @ z1 + s2 @ z2) / max(1.0, abs(F)))
         info = dict(gap=gap, kkt=kkt, obj=0.5 * bQb - bb + lam * c.sum(), lasso_obj=F, mu=mu,
                     dual_inf=np.abs(rd).max(), ipm_iter=k, cg_iter=tot_cg)
         if verbose:
