@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--workload", default="3d320", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     return ap.parse_args()
 
 
@@ -269,15 +270,17 @@ def run_ours(args):
         torch.cuda.current_stream().synchronize()
         L.csipm_destroy(h)
 
-    e2e_step()   # warm
-    D.barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = D.max(e0.elapsed_time(e1) / args.steps)
+    e2e_ms = float("nan")
+    if not args.no_e2e:
+        e2e_step()   # warm
+        D.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = D.max(e0.elapsed_time(e1) / args.steps)
 
     # ---- roofline of the dominant kernel (each pass timed alone, CUDA events)
     ms_p = (ctypes.c_double * 8)()

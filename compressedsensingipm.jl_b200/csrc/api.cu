@@ -134,7 +134,9 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
     h->bytes += h->op64.bytes;
     // reduction workspace: enough partials for the largest grid
-    size_t maxblocks = 4096;
+    size_t maxblocks = 8192;
+    if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * (h->g.dim == 3 ? h->g.n3 : 1));
+    if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * h->g.n2);
     maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.row_cfg.grid.x);
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s2_cfg.grid.x * h->op64.s2_cfg.grid.y);
     if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s3_cfg.grid.x * h->op64.s3_cfg.grid.y);
@@ -362,35 +364,34 @@ int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_o
     };
     int r = 0;
     if (g.dim == 1) {
-        r = timeit([&] { return mask ? launch_row<double, IN_GATHER, OUT_SCATTER, true>(op.row_cfg, ra, x, ecg, st)
-                                     : launch_row<double, IN_GATHER, OUT_SCATTER, false>(op.row_cfg, ra, x, ecg, st); },
+        r = timeit([&] { return mask ? run_row<double, IN_GATHER, OUT_SCATTER, true>(op, ra, x, ecg, st)
+                                     : run_row<double, IN_GATHER, OUT_SCATTER, false>(op, ra, x, ecg, st); },
                    4 * w * N + maskb, "row: gather+C2R+mask+R2C+scatter+CG");
         if (r) return r;
     } else {
-        const int ax = g.dim;   // outermost axis
-        PassArgs<double> ao = op.strided_args(ax);
-        const PassCfg& co = ax == 3 ? op.s3_cfg : op.s2_cfg;
-        r = timeit([&] { return launch_strided<double, true, IN_GATHER, OUT_SPEC>(co, ao, x, none, st); },
-                   w * N + cw * Nh, ax == 3 ? "gather+inverse dim3" : "gather+inverse dim2");
+        // same order as the product: beta-side passes along dim 2, plain ones along dim 3
+        PassArgs<double> a2 = op.strided_args(2);
+        r = timeit([&] { return run_strided<double, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st); },
+                   w * N + cw * Nh, "gather+inverse dim2");
         if (r) return r;
         if (g.dim == 3) {
-            PassArgs<double> a2 = op.strided_args(2);
-            r = timeit([&] { return launch_strided<double, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st); },
-                       2 * cw * Nh, "inverse dim2");
+            PassArgs<double> a3 = op.strided_args(3);
+            r = timeit([&] { return run_strided<double, true, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
+                       2 * cw * Nh, "inverse dim3");
             if (r) return r;
         }
-        r = timeit([&] { return mask ? launch_row<double, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
-                                     : launch_row<double, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st); },
+        r = timeit([&] { return mask ? run_row<double, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
+                                     : run_row<double, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st); },
                    2 * cw * Nh + maskb, "row: C2R+mask+R2C dim1");
         if (r) return r;
         if (g.dim == 3) {
-            PassArgs<double> a2 = op.strided_args(2);
-            r = timeit([&] { return launch_strided<double, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st); },
-                       2 * cw * Nh, "forward dim2");
+            PassArgs<double> a3 = op.strided_args(3);
+            r = timeit([&] { return run_strided<double, false, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
+                       2 * cw * Nh, "forward dim3");
             if (r) return r;
         }
-        r = timeit([&] { return launch_strided<double, false, IN_SPEC, OUT_SCATTER>(co, ao, (const double*)nullptr, ecg, st); },
-                   cw * Nh + 3 * w * N, ax == 3 ? "forward dim3+scatter+CG" : "forward dim2+scatter+CG");
+        r = timeit([&] { return run_strided<double, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, ecg, st); },
+                   cw * Nh + 3 * w * N, "forward dim2+scatter+CG");
         if (r) return r;
     }
     *npass = np;

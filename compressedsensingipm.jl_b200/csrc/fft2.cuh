@@ -1,0 +1,307 @@
+// Two-level register FFT passes: L = A*B.
+//
+// Step 1: each thread owns one residue t < B of a line and loads its A
+// elements x[t + B*a] straight from global memory into registers (A loads in
+// flight per thread), runs DFT_A, multiplies by W_L^{t*ka} and writes the A
+// results to shared memory.  Step 2: thread s < A reads its B values, runs
+// DFT_B and owns the outputs X[s + A*kb].  One shared-memory round trip per
+// transform (the Stockham engine needs one per radix stage).
+//
+// In the row pass the inverse transform (A, B) leaves thread s with
+// z[s + A*kb]; the forward transform is run with the factors swapped (B, A),
+// whose first step wants exactly those elements, so C2R -> mask -> R2C costs
+// two exchanges plus one for the R2C post-processing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft_device.cuh"
+#include "operator.cuh"
+
+namespace csipm {
+
+constexpr int FFT2_TB = 8;      // lines per CTA of the strided two-level pass (FP64: 128 B per access)
+
+// twiddle of the strided pass: W_L^e (forward) from a table of L-th roots
+template <bool INV, typename C>
+__device__ __forceinline__ C tw_apply(C v, const C* __restrict__ tw, int e) {
+    if (e == 0) return v;
+    const C w = tw[e];
+    return INV ? cmulc(v, w) : cmul(v, w);
+}
+
+// ------------------------------------------------------------ strided pass
+template <typename T, int A, int B, bool INV, int IN, int OUT, typename TS, class Epi>
+__global__ void __launch_bounds__(FFT2_TB * (A > B ? A : B))
+strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    using C = cplx_t<T>;
+    constexpr int TB = FFT2_TB;
+    constexpr int L = A * B;
+    if (a.skip && *a.skip) return;
+    __shared__ C S[L * TB];
+    const int b = threadIdx.x % TB, t = threadIdx.x / TB;
+    const int i0 = blockIdx.x * TB, o = blockIdx.y;
+    const int nb = min(TB, a.n_lines - i0);
+    const bool live = b < nb;
+    const long long base = i0 + b + (long long)o * a.so;
+    const C* __restrict__ tw = a.tw;    // L-th roots (Ltab == L)
+    const C zero = mk((T)0, (T)0);
+    // each thread keeps one dim-1 position for the whole tile: interior
+    // positions (all but i = 0 and i = M1) take the short decode
+    const int ii = i0 + b;
+    const bool interior = ii >= 1 && ii <= a.g.m1 - 1;
+
+    // ---- step 1: thread t < B owns x = t + B*a
+    if (t < B) {
+        C v[A];
+#pragma unroll
+        for (int q = 0; q < A; ++q) {
+            const int x = t + B * q;
+            if (!live) {
+                v[q] = zero;
+            } else if (IN == IN_SPEC) {
+                v[q] = a.spec[base + (long long)x * a.sx];
+            } else {
+                int j, k;
+                jk_of(a.jk_mode, o, x, j, k);
+                const MapEntry en = interior ? decode_interior(a.g, ii, j, k) : decode(a.g, ii, j, k);
+                v[q] = gather_val<T>(en, src);
+            }
+        }
+        Dft<A, INV, T>::run(v);
+#pragma unroll
+        for (int ka = 0; ka < A; ++ka) S[(ka * B + t) * TB + b] = tw_apply<INV>(v[ka], tw, t * ka);
+    }
+    __syncthreads();
+    // ---- step 2: thread s < A owns X[s + A*kb]
+    Epi ep = epi;
+    if (t < A && live) {
+        const int s = t;
+        C u[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q) u[q] = S[(s * B + q) * TB + b];
+        Dft<B, INV, T>::run(u);
+        if (OUT == OUT_SPEC) {
+#pragma unroll
+            for (int kb = 0; kb < B; ++kb) a.spec[base + (long long)(s + A * kb) * a.sx] = u[kb];
+        } else {
+            constexpr int U = 2;
+#pragma unroll
+            for (int k0 = 0; k0 < B; k0 += U) {
+                MapEntry en[U];
+                typename Epi::Pre pr[U], pi[U];
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    if (k0 + q < B) {
+                        int j, k;
+                        jk_of(a.jk_mode, o, s + A * (k0 + q), j, k);
+                        en[q] = interior ? decode_interior(a.g, ii, j, k) : decode(a.g, ii, j, k);
+                        if (en[q].src) {
+                            pr[q] = ep.pre(en[q].re);
+                            if (en[q].kind != KIND_VERT) pi[q] = ep.pre(en[q].im);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    if (k0 + q < B && en[q].src) {
+                        const C v = u[k0 + q];
+                        if (en[q].kind == KIND_VERT) {
+                            ep.put(en[q].re, (double)v.x, pr[q]);
+                        } else {
+                            ep.put(en[q].re, SQRT2_D * (double)v.x, pr[q]);
+                            ep.put(en[q].im, (en[q].kind == KIND_PLUS ? SQRT2_D : -SQRT2_D) * (double)v.y, pi[q]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (OUT == OUT_SCATTER) ep.finish();
+}
+
+// ---------------------------------------------------------------- row pass
+// M = A*B half-spectrum length (dim-1 complex FFT length); rows of M+1 values.
+template <typename T, int A, int B> struct Row2Shape {
+    static constexpr int M = A * B;
+    static constexpr int X1 = A * (B + 1);          // inverse exchange  [ka][t],  t-stride 1, ka-stride B+1
+    static constexpr int X2 = B * (A + 1);          // forward exchange  [kb][s],  s-stride 1, kb-stride A+1
+    static constexpr int XC = X1 > X2 ? X1 : X2;
+    static constexpr int PER_ROW = XC + M + 1;      // exchange area + natural-order spectrum for R2C post
+    // rows per CTA: as many as fit in 48 KB of static shared memory, at most 8
+    static constexpr int R0 = (48 * 1024) / (PER_ROW * (int)sizeof(cplx_t<T>));
+    static constexpr int ROWS = R0 > 8 ? 8 : (R0 < 1 ? 1 : R0);
+    static constexpr int NTL = A > B ? A : B;
+};
+
+template <typename T, int A, int B, int IN, int OUT, bool MASK>
+__global__ void __launch_bounds__(Row2Shape<T, A, B>::ROWS * Row2Shape<T, A, B>::NTL)
+row2_kernel(PassArgs<T> a) {
+    using C = cplx_t<T>;
+    using Sh = Row2Shape<T, A, B>;
+    constexpr int M = Sh::M;
+    constexpr int NTL = Sh::NTL;
+    if (a.skip && *a.skip) return;
+    __shared__ C S[Sh::ROWS * Sh::PER_ROW];
+    const int r = threadIdx.x / NTL, t = threadIdx.x % NTL;
+    const int row = blockIdx.x * Sh::ROWS + r;
+    const bool live = row < a.nrows;
+    C* X = S + r * Sh::PER_ROW;           // exchange area of this row
+    C* P = X + Sh::XC;                    // natural-order spectrum (R2C post)
+    const C* __restrict__ tw = a.tw;      // N1-th roots, W_M^e = tw[2e]
+    const C zero = mk((T)0, (T)0);
+    const T sc = (T)a.scale;
+
+    // z[s + A*kb] for the thread s < A after the inverse transform (or the load)
+    C z[B];
+    if (IN == IN_REAL) {
+        if (t < A) {
+#pragma unroll
+            for (int kb = 0; kb < B; ++kb) {
+                const int n = t + A * kb;
+                z[kb] = live ? *reinterpret_cast<const C*>(a.real_in + (size_t)row * a.g.n1 + 2 * n) : zero;
+            }
+        }
+    } else {
+        // ---- inverse step 1 (thread t < B): C2R pre-processing at load
+        if (t < B) {
+            C v[A];
+            const C* rowp = a.spec + (size_t)row * a.g.ld1;
+#pragma unroll
+            for (int q = 0; q < A; ++q) {
+                const int x = t + B * q;
+                if (live) {
+                    const C xa = rowp[x], xb = rowp[M - x];
+                    v[q] = c2r_pre(xa, xb, tw[x]);
+                } else {
+                    v[q] = zero;
+                }
+            }
+            Dft<A, true, T>::run(v);
+#pragma unroll
+            for (int ka = 0; ka < A; ++ka) {
+                C w = v[ka];
+                const int e = t * ka;
+                if (e) w = cmulc(w, tw[2 * e]);
+                X[ka * (B + 1) + t] = w;
+            }
+        }
+        __syncthreads();
+        // ---- inverse step 2 (thread s < A)
+        if (t < A) {
+#pragma unroll
+            for (int q = 0; q < B; ++q) z[q] = X[t * (B + 1) + q];
+            Dft<B, true, T>::run(z);
+        }
+        __syncthreads();   // X is reused by the forward exchange
+    }
+    // ---- scale and mask the real samples (x[2n], x[2n+1]) = z[n], n = s + A*kb
+    if (t < A) {
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) {
+            const int n = t + A * kb;
+            C y = z[kb];
+            y.x *= sc;
+            y.y *= sc;
+            if (MASK && live) {
+                const uint32_t w = a.maskw[(size_t)row * a.wpr + (n >> 4)];
+                const int sh = (2 * n) & 31;
+                if (!((w >> sh) & 1u)) y.x = (T)0;
+                if (!((w >> (sh + 1)) & 1u)) y.y = (T)0;
+            }
+            z[kb] = y;
+            if (OUT == OUT_REAL && live) *reinterpret_cast<C*>(a.real_out + (size_t)row * a.g.n1 + 2 * n) = y;
+        }
+    }
+    if (OUT == OUT_REAL) return;
+    // ---- forward transform with factors (B, A): step 1 on the thread's own z
+    if (t < A) {
+        Dft<B, false, T>::run(z);
+#pragma unroll
+        for (int kb = 0; kb < B; ++kb) {
+            C w = z[kb];
+            const int e = t * kb;
+            if (e) w = cmul(w, tw[2 * e]);
+            X[kb * (A + 1) + t] = w;
+        }
+    }
+    __syncthreads();
+    // step 2 (thread t < B): outputs Z[t + B*ka]
+    if (t < B) {
+        C u[A];
+#pragma unroll
+        for (int q = 0; q < A; ++q) u[q] = X[t * (A + 1) + q];
+        Dft<A, false, T>::run(u);
+#pragma unroll
+        for (int ka = 0; ka < A; ++ka) P[t + B * ka] = u[ka];
+    }
+    __syncthreads();
+    // ---- R2C post-processing and coalesced store of the M+1 values
+    if (live) {
+        C* rowp = a.spec + (size_t)row * a.g.ld1;
+        for (int k = t; k <= M; k += NTL) {
+            if (k == 0 || k == M) {
+                const C z0 = P[0];
+                rowp[k] = k == 0 ? r2c_post(z0, z0, tw[0]) : mk((T)2 * (z0.x - z0.y), (T)0);
+            } else {
+                rowp[k] = r2c_post(P[k], P[M - k], tw[k]);
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------- dispatch
+// Factor L = A*B for the two-level passes (A, B <= 20, A <= B, balanced);
+// returns false when L has no supported factorisation.
+inline bool fft2_factor(int L, int* A, int* B) {
+    static const int sup[] = {20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
+    int bestA = 0, bestB = 0;
+    for (int b : sup) {
+        if (L % b) continue;
+        const int a = L / b;
+        bool ok = false;
+        for (int s : sup) ok |= (s == a);
+        if (!ok || a > b) continue;
+        if (!bestA || a > bestA) { bestA = a; bestB = b; }
+    }
+    if (!bestA) return false;
+    *A = bestA;
+    *B = bestB;
+    return true;
+}
+
+// The (A, B) pairs the library instantiates (fft2.cu).
+inline bool fft2_strided_pair(int A, int B) {
+    return (A == 16 && B == 20) || (A == 16 && B == 16) || (A == 10 && B == 16) || (A == 8 && B == 16) ||
+           (A == 8 && B == 8);
+}
+inline bool fft2_row_pair(int A, int B) {
+    return (A == 10 && B == 16) || (A == 8 && B == 16) || (A == 8 && B == 10) || (A == 8 && B == 8) ||
+           (A == 16 && B == 16);
+}
+
+template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
+cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st);
+
+template <typename T, int IN, int OUT, bool MASK>
+cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st);
+
+// epilogues the two-level strided pass is instantiated with
+template <class Epi> struct Fft2Epi { static constexpr bool value = false; };
+template <> struct Fft2Epi<EpiStore<double>> { static constexpr bool value = true; };
+template <> struct Fft2Epi<EpiCG<double>> { static constexpr bool value = true; };
+
+}  // namespace csipm
+
+namespace csipm {
+
+template <typename T>
+inline void FftOperator<T>::choose_two_level() {
+    s2_A = s2_B = s3_A = s3_B = r_A = r_B = 0;
+    if (sizeof(T) != 8 || g.dim < 2) return;
+    int A = 0, B = 0;
+    if (fft2_factor(g.n2, &A, &B) && fft2_strided_pair(A, B)) { s2_A = A; s2_B = B; }
+    if (g.dim == 3 && fft2_factor(g.n3, &A, &B) && fft2_strided_pair(A, B)) { s3_A = A; s3_B = B; }
+    if (fft2_factor(g.m1, &A, &B) && fft2_row_pair(A, B)) { r_A = A; r_B = B; }
+}
+
+}  // namespace csipm

@@ -184,6 +184,47 @@ CSIPM_HD MapEntry decode3(const Geom& g, int i, int j, int k) {
     return flip ? flip_entry(e) : e;
 }
 
+// Decode for an interior dim-1 position (1 <= i <= M1-1, half spectrum), the
+// case of all but two of every M1+1 positions: no mirror flip, no vertex,
+// edge-along-k, edge-along-j or face-i branches.
+CSIPM_HD MapEntry decode_interior(const Geom& g, int i, int j, int k) {
+    MapEntry e;
+    const int ti = i - 1, tm = g.m1 - i - 1;
+    e.src = 1;
+    if (g.dim == 2) {
+        const int cj = coord_class(j, g.m2);
+        e.kind = KIND_PLUS;
+        if (cj <= 1) { e.re = g.o2E1 + 2 * cj * g.p1 + ti; e.im = e.re + g.p1; }
+        else if (cj == 2) { e.re = g.o2C + (j - 1) * g.p1 + ti; e.im = e.re + g.PP; }
+        else { e.re = g.o2C + 2 * g.PP + (j - g.m2 - 1) * g.p1 + ti; e.im = e.re + g.PP; }
+        return e;
+    }
+    if (g.dim == 1) { e.re = i + 1; e.im = g.m1 + i; e.kind = KIND_PLUS; return e; }
+    const int cj = coord_class(j, g.m2), ck = coord_class(k, g.m3);
+    if (cj <= 1 && ck <= 1) {
+        e.re = g.oE1 + 2 * (2 * cj + ck) * g.p1 + ti; e.im = e.re + g.p1; e.kind = KIND_PLUS;
+    } else if (cj <= 1) {
+        const int o = g.oFj + 4 * cj * g.P13;
+        if (ck == 2) { e.re = o + (k - 1) * g.p1 + ti; e.kind = KIND_PLUS; }
+        else { e.re = o + 2 * g.P13 + (g.n3 - k - 1) * g.p1 + tm; e.kind = KIND_MINUS; }
+        e.im = e.re + g.P13;
+    } else if (ck <= 1) {
+        const int o = g.oFk + 4 * ck * g.P12;
+        if (cj == 2) { e.re = o + (j - 1) * g.p1 + ti; e.kind = KIND_PLUS; }
+        else { e.re = o + 2 * g.P12 + (g.n2 - j - 1) * g.p1 + tm; e.kind = KIND_MINUS; }
+        e.im = e.re + g.P12;
+    } else if (cj == 2 && ck == 2) {
+        e.re = g.oC + (k - 1) * g.P12 + (j - 1) * g.p1 + ti; e.im = e.re + g.P123; e.kind = KIND_PLUS;
+    } else if (cj == 3 && ck == 3) {
+        e.re = g.oC + 2 * g.P123 + (g.n3 - k - 1) * g.P12 + (g.n2 - j - 1) * g.p1 + tm; e.im = e.re + g.P123; e.kind = KIND_MINUS;
+    } else if (cj == 3) {
+        e.re = g.oC + 4 * g.P123 + (k - 1) * g.P12 + (j - g.m2 - 1) * g.p1 + ti; e.im = e.re + g.P123; e.kind = KIND_PLUS;
+    } else {
+        e.re = g.oC + 6 * g.P123 + (g.n3 - k - 1) * g.P12 + (g.m2 - j - 1) * g.p1 + tm; e.im = e.re + g.P123; e.kind = KIND_MINUS;
+    }
+    return e;
+}
+
 CSIPM_HD MapEntry decode(const Geom& g, int i, int j, int k) {
     return g.dim == 3 ? decode3(g, i, j, k) : (g.dim == 2 ? decode2(g, i, j) : decode1(g, i));
 }

@@ -13,8 +13,10 @@
 
 #include "../../include/csipm.h"
 #include "geometry.h"
+#include "fft2.cuh"
 #include "operator.cuh"
 #include "solver_kernels.cuh"
+#include <type_traits>
 
 namespace csipm {
 void set_last_error(const std::string& msg);
@@ -143,6 +145,31 @@ inline int fail(csipm_handle h, int status, const std::string& msg) {
 // slot indices in h->slots
 enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_COUNT = 64 };
 
+// ------------------------------------------------------------------ pass dispatch
+// Strided pass along `axis`: the two-level register kernel when the axis has
+// an instantiated factor pair and the epilogue is a hot-path one, else the
+// persistent Stockham kernel.
+template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
+cudaError_t run_strided(FftOperator<T>& op, int axis, const PassArgs<T>& a, const TS* src, const Epi& epi,
+                        cudaStream_t st) {
+    if constexpr (Fft2Epi<Epi>::value && std::is_same<T, double>::value && std::is_same<TS, double>::value) {
+        const int A = axis == 3 ? op.s3_A : op.s2_A, B = axis == 3 ? op.s3_B : op.s2_B;
+        if (A) return launch_strided2<T, INV, IN, OUT, TS, Epi>(A, B, a, src, epi, st);
+    }
+    return launch_strided<T, INV, IN, OUT>(axis == 3 ? op.s3_cfg : op.s2_cfg, a, src, epi, st);
+}
+
+// Row pass: the two-level kernel for 2D/3D spectrum/real passes with an
+// instantiated factor pair, else the Stockham kernel (also all 1D passes).
+template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
+cudaError_t run_row(FftOperator<T>& op, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
+    if constexpr (std::is_same<T, double>::value && IN != IN_GATHER && OUT != OUT_SCATTER &&
+                  !(IN == IN_REAL && OUT == OUT_REAL) && !(IN == IN_REAL && MASK)) {
+        if (op.r_A && op.g.dim >= 2) return launch_row2<T, IN, OUT, MASK>(op.r_A, op.r_B, a, st);
+    }
+    return launch_row<T, IN, OUT, MASK>(op.row_cfg, a, src, epi, st);
+}
+
 // ------------------------------------------------------------------ operator
 template <typename T, typename TS, class Epi>
 cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* skip, cudaStream_t st) {
@@ -154,32 +181,34 @@ cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* s
     PassArgs<T> ra = op.row_args(sc, nullptr, nullptr);
     ra.skip = skip;
     if (g.dim == 1) {
-        return mask ? launch_row<T, IN_GATHER, OUT_SCATTER, true>(op.row_cfg, ra, x, epi, st)
-                    : launch_row<T, IN_GATHER, OUT_SCATTER, false>(op.row_cfg, ra, x, epi, st);
+        return mask ? run_row<T, IN_GATHER, OUT_SCATTER, true>(op, ra, x, epi, st)
+                    : run_row<T, IN_GATHER, OUT_SCATTER, false>(op, ra, x, epi, st);
     }
     if (g.dim == 2) {
         PassArgs<T> a2 = op.strided_args(2);
         a2.skip = skip;
-        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s2_cfg, a2, x, none, st);
+        e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st);
         if (e != cudaSuccess) return e;
-        e = mask ? launch_row<T, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
-                 : launch_row<T, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+        e = mask ? run_row<T, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
+                 : run_row<T, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st);
         if (e != cudaSuccess) return e;
-        return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s2_cfg, a2, (const double*)nullptr, epi, st);
+        return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, epi, st);
     }
+    // 3D: the beta-side passes run along dim 2 (line stride N1/2+1 elements),
+    // the plain spectrum passes along dim 3 (stride (N1/2+1)*N2)
     PassArgs<T> a3 = op.strided_args(3), a2 = op.strided_args(2);
     a3.skip = skip;
     a2.skip = skip;
-    e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s3_cfg, a3, x, none, st);
+    e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st);
     if (e != cudaSuccess) return e;
-    e = launch_strided<T, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st);
+    e = run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    e = mask ? launch_row<T, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
-             : launch_row<T, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+    e = mask ? run_row<T, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
+             : run_row<T, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    e = launch_strided<T, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, st);
+    e = run_strided<T, false, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s3_cfg, a3, (const double*)nullptr, epi, st);
+    return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, epi, st);
 }
 
 // x = P(sqrt(N) Re ifft(B beta))
@@ -191,18 +220,18 @@ cudaError_t op_A(FftOperator<T>& op, const TS* beta, T* x, cudaStream_t st) {
     PassArgs<T> ra = op.row_args(1.0 / std::sqrt((double)g.N), nullptr, x);
     cudaError_t e;
     if (g.dim == 1)
-        return mask ? launch_row<T, IN_GATHER, OUT_REAL, true>(op.row_cfg, ra, beta, none, st)
-                    : launch_row<T, IN_GATHER, OUT_REAL, false>(op.row_cfg, ra, beta, none, st);
+        return mask ? run_row<T, IN_GATHER, OUT_REAL, true>(op, ra, beta, none, st)
+                    : run_row<T, IN_GATHER, OUT_REAL, false>(op, ra, beta, none, st);
     if (g.dim == 3) {
-        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s3_cfg, op.strided_args(3), beta, none, st);
+        e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, op.strided_args(2), beta, none, st);
         if (e != cudaSuccess) return e;
-        e = launch_strided<T, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, none, st);
+        e = run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 3, op.strided_args(3), (const double*)nullptr, none, st);
     } else {
-        e = launch_strided<T, true, IN_GATHER, OUT_SPEC>(op.s2_cfg, op.strided_args(2), beta, none, st);
+        e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, op.strided_args(2), beta, none, st);
     }
     if (e != cudaSuccess) return e;
-    return mask ? launch_row<T, IN_SPEC, OUT_REAL, true>(op.row_cfg, ra, (const double*)nullptr, none, st)
-                : launch_row<T, IN_SPEC, OUT_REAL, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+    return mask ? run_row<T, IN_SPEC, OUT_REAL, true>(op, ra, (const double*)nullptr, none, st)
+                : run_row<T, IN_SPEC, OUT_REAL, false>(op, ra, (const double*)nullptr, none, st);
 }
 
 // beta = B^T(fft(z)/sqrt(N)) through the epilogue
@@ -212,13 +241,13 @@ cudaError_t op_At(FftOperator<T>& op, const T* z, const Epi& epi, cudaStream_t s
     EpiStore<double> none{nullptr};
     PassArgs<T> ra = op.row_args(1.0 / (2.0 * std::sqrt((double)g.N)), z, nullptr);
     cudaError_t e;
-    if (g.dim == 1) return launch_row<T, IN_REAL, OUT_SCATTER, false>(op.row_cfg, ra, (const double*)nullptr, epi, st);
-    e = launch_row<T, IN_REAL, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, st);
+    if (g.dim == 1) return run_row<T, IN_REAL, OUT_SCATTER, false>(op, ra, (const double*)nullptr, epi, st);
+    e = run_row<T, IN_REAL, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    if (g.dim == 2) return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, epi, st);
-    e = launch_strided<T, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, op.strided_args(2), (const double*)nullptr, none, st);
+    if (g.dim == 2) return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, op.strided_args(2), (const double*)nullptr, epi, st);
+    e = run_strided<T, false, IN_SPEC, OUT_SPEC>(op, 3, op.strided_args(3), (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    return launch_strided<T, false, IN_SPEC, OUT_SCATTER>(op.s3_cfg, op.strided_args(3), (const double*)nullptr, epi, st);
+    return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, op.strided_args(2), (const double*)nullptr, epi, st);
 }
 
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }

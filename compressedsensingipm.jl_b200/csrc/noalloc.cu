@@ -134,19 +134,19 @@ int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, 
         e = mask ? launch_row<double, IN_GATHER, OUT_SCATTER, true>(op.row_cfg, ra, x, out, s)
                  : launch_row<double, IN_GATHER, OUT_SCATTER, false>(op.row_cfg, ra, x, out, s);
     } else {
-        const PassCfg& co = dim == 3 ? op.s3_cfg : op.s2_cfg;
-        PassArgs<double> ao = op.strided_args(dim);
+        // beta-side passes along dim 2, plain spectrum passes along dim 3
         PassArgs<double> a2 = op.strided_args(2);
-        e = launch_strided<double, true, IN_GATHER, OUT_SPEC>(co, ao, x, none, s);
+        PassArgs<double> a3 = dim == 3 ? op.strided_args(3) : a2;
+        e = launch_strided<double, true, IN_GATHER, OUT_SPEC>(op.s2_cfg, a2, x, none, s);
         if (e == cudaSuccess && dim == 3)
-            e = launch_strided<double, true, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, s);
+            e = launch_strided<double, true, IN_SPEC, OUT_SPEC>(op.s3_cfg, a3, (const double*)nullptr, none, s);
         if (e == cudaSuccess)
             e = mask ? launch_row<double, IN_SPEC, OUT_SPEC, true>(op.row_cfg, ra, (const double*)nullptr, none, s)
                      : launch_row<double, IN_SPEC, OUT_SPEC, false>(op.row_cfg, ra, (const double*)nullptr, none, s);
         if (e == cudaSuccess && dim == 3)
-            e = launch_strided<double, false, IN_SPEC, OUT_SPEC>(op.s2_cfg, a2, (const double*)nullptr, none, s);
+            e = launch_strided<double, false, IN_SPEC, OUT_SPEC>(op.s3_cfg, a3, (const double*)nullptr, none, s);
         if (e == cudaSuccess)
-            e = launch_strided<double, false, IN_SPEC, OUT_SCATTER>(co, ao, (const double*)nullptr, out, s);
+            e = launch_strided<double, false, IN_SPEC, OUT_SCATTER>(op.s2_cfg, a2, (const double*)nullptr, out, s);
     }
     if (e != cudaSuccess) return static_fail(CSIPM_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
     return CSIPM_OK;

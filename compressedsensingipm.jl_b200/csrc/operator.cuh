@@ -584,6 +584,8 @@ public:
     C* tw2 = nullptr;
     C* tw3 = nullptr;
     PassCfg row_cfg, s2_cfg, s3_cfg;
+    // two-level register passes (fft2.cuh): factor pairs, 0 when not used
+    int s2_A = 0, s2_B = 0, s3_A = 0, s3_B = 0, r_A = 0, r_B = 0;
     size_t bytes = 0;
     bool owns = true;               // false: buffers belong to someone else; release() frees nothing
 
@@ -686,6 +688,10 @@ public:
     // complex values per thread, FP32 32)
     static int max_radix() { return 8; }
 
+    // Use the two-level register passes where the line length factors into an
+    // instantiated pair (FP64, 2D/3D).
+    void choose_two_level();
+
     bool make_plans(std::string* err) {
         if (!make_fft_plan(g.m1, &plan1, err, max_radix())) return false;
         if (g.dim >= 2 && !make_fft_plan(g.n2, &plan2, err, max_radix())) return false;
@@ -699,6 +705,7 @@ public:
         if (!make_plans(err)) return false;
         const int nrows = g.n2 * g.n3;
         if (!choose_row(nrows, &row_cfg, err)) return false;
+        choose_two_level();
         if (g.dim >= 2 && !choose_strided(plan2, g.n2, g.m1 + 1, g.dim == 3 ? g.n3 : 1, &s2_cfg, err)) return false;
         if (g.dim >= 3 && !choose_strided(plan3, g.n3, g.m1 + 1, g.n2, &s3_cfg, err)) return false;
         if (!upload_table(g.n1, &tw1, err)) return false;
