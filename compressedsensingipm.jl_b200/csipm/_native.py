@@ -62,6 +62,7 @@ class Options(ctypes.Structure):
         ("ir_max", ctypes.c_int),
         ("verbose", ctypes.c_int),
         ("stream", ctypes.c_void_p),
+        ("layout", ctypes.c_int),
     ]
 
 

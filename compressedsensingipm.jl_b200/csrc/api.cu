@@ -16,6 +16,48 @@ const char* get_last_error() { return g_last_error.c_str(); }
 
 namespace csipm_internal {
 
+// ------------------------------------------------------------------ solver order
+// One thread per solver-order pair (NI of them) and per tail entry; every
+// reference index is read or written exactly once (the packing is a bijection
+// between beta entries and the sources of the half spectrum).
+template <bool TO_SOL>
+static __global__ void solver_order_kernel(Geom g, const double* __restrict__ in, double* __restrict__ out) {
+    const int64_t tail = g.N - 2 * g.NI;
+    const int64_t total = g.NI + tail;
+    const int pl = g.m1 - 1;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        if (idx < g.NI) {
+            const int i = (int)(idx % pl) + 1;
+            const int64_t r = idx / pl;
+            const int j = (int)(r % g.n2), k = (int)(r / g.n2);
+            const MapEntry e = decode_interior(g, i, j, k);
+            const double sg = e.kind == KIND_MINUS ? -1.0 : 1.0;
+            if (TO_SOL) {
+                reinterpret_cast<double2*>(out)[idx] = make_double2(in[e.re], sg * in[e.im]);
+            } else {
+                const double2 v = reinterpret_cast<const double2*>(in)[idx];
+                out[e.re] = v.x;
+                out[e.im] = sg * v.y;
+            }
+        } else {
+            const int64_t t = idx - g.NI;
+            const int64_t ref = sol_tail_ref(g, t);
+            if (TO_SOL) out[2 * g.NI + t] = in[ref];
+            else out[ref] = in[2 * g.NI + t];
+        }
+    }
+}
+
+cudaError_t to_solver_order(const Geom& g, const double* ref, double* sol, cudaStream_t st) {
+    solver_order_kernel<true><<<ew_blocks(g.N / 2 + 1), EW_THREADS, 0, st>>>(g, ref, sol);
+    return cudaGetLastError();
+}
+
+cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cudaStream_t st) {
+    solver_order_kernel<false><<<ew_blocks(g.N / 2 + 1), EW_THREADS, 0, st>>>(g, sol, ref);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ Schur PCG
 // Solves (A'A + Db) x = rhs with preconditioner Minv (csipm_solve's inner solve).
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
@@ -27,7 +69,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
     const int ppp = passes_per_product(h->g);
     if (has_x0) {
         EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
-        CK(op_AtA(h->op64, x, ep, nullptr, st));
+        CK(solve_AtA(h, x, ep, nullptr, st));
         h->matvecs++;
         h->launches += ppp;
     } else {
@@ -42,7 +84,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
     int since = 0;
     for (; it < maxit; ++it) {
         EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
-        CK(op_AtA(h->op64, h->cg_p, ep, &h->cgs->done, st));
+        CK(solve_AtA(h, h->cg_p, ep, &h->cgs->done, st));
         cg_update_kernel<double, double><<<nb, EW_THREADS, 0, st>>>(n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
                                                                     h->ws(h->slots + SL_DUMMY), h->cgs);
         cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, it, h->cg_r, Minv, h->cg_p, h->cgs);
@@ -167,6 +209,13 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         cudaStreamSynchronize(h->stream) != cudaSuccess)
         return bail(CSIPM_ERR_CUDA, "synchronisation failed after A^T z0");
     h->z0sq = h->hslots[SL_DOT];
+    if (h->opt.layout == 0 && solver_order_ok(h->op64)) {
+        if (!h->alloc(&h->bs, n_)) return bail(CSIPM_ERR_OOM, h->err);
+        if (to_solver_order(h->g, h->b, h->bs, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bail(CSIPM_ERR_CUDA, "solver-order copy of A^T z0 failed");
+        h->sorder = true;
+    }
     *out = h;
     return CSIPM_OK;
 }
@@ -226,16 +275,18 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     const long long la0 = h->launches;
     const int ppp = passes_per_product(h->g);
     cudaEventRecord(h->ev0, st);
+    // every beta-space vector of the solve is in solver order when h->sorder
+    const double* bv = h->sorder ? h->bs : h->b;
     // ---- initial point: beta = soft(A^T z0, lambda), z from the clipped gradient, c balanced
-    ipm_init1_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->b, lam, h->beta, h->ws(h->slots + SL_MAXB));
+    ipm_init1_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, lam, h->beta, h->ws(h->slots + SL_MAXB));
     CK(cudaGetLastError());
     {
         EpiStore<double> ep{h->Qb};
-        CK(op_AtA(h->op64, h->beta, ep, nullptr, st));
+        CK(solve_AtA(h, h->beta, ep, nullptr, st));
         h->matvecs++;
     }
     h->launches += 2 + ppp;
-    ipm_init2_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->b, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->c, h->z1, h->z2);
+    ipm_init2_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->c, h->z1, h->z2);
     CK(cudaGetLastError());
     {
         int r0 = read_slots(h, SL_MAXB, 2);
@@ -248,12 +299,12 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     for (;; ++k) {
         if (k > 0) {
             EpiStore<double> ep{h->Qb};
-            CK(op_AtA(h->op64, h->beta, ep, nullptr, st));
+            CK(solve_AtA(h, h->beta, ep, nullptr, st));
             h->matvecs++;
             h->launches += ppp;
         }
         h->launches += 1;   // residual
-        ipm_residual_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->b, h->Qb, lam, h->beta, h->c, h->z1, h->z2, h->rd,
+        ipm_residual_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->c, h->z1, h->z2, h->rd,
                                                        h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
         int r = read_slots(h, SL_RED, RR_N);
@@ -317,8 +368,14 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         CK(cudaGetLastError());
         h->launches += 7;   // diag, 2 rhs, 2 step statistics, update (+ CG launches counted in schur_cg)
     }
-    CK(cudaMemcpyAsync(beta_out, h->beta, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    if (c_out) CK(cudaMemcpyAsync(c_out, h->c, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    if (h->sorder) {
+        CK(to_reference_order(h->g, h->beta, beta_out, st));
+        if (c_out) CK(to_reference_order(h->g, h->c, c_out, st));
+        h->launches += c_out ? 2 : 1;
+    } else {
+        CK(cudaMemcpyAsync(beta_out, h->beta, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        if (c_out) CK(cudaMemcpyAsync(c_out, h->c, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    }
     cudaEventRecord(h->ev1, st);
     CK(cudaEventSynchronize(h->ev1));
     float ms = 0.f;
@@ -371,7 +428,11 @@ int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_o
     } else {
         // same order as the product: beta-side passes along dim 2, plain ones along dim 3
         PassArgs<double> a2 = op.strided_args(2);
-        r = timeit([&] { return run_strided<double, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st); },
+        // (the solve's order: solver-order gather/scatter when the handle uses it)
+        const bool so = h->sorder;
+        if (so && !aligned16(x)) return fail(h, CSIPM_ERR_INVALID, "x must be 16-byte aligned");
+        r = timeit([&] { return so ? run_strided<double, true, IN_SGATHER, OUT_SPEC>(op, 2, a2, x, none, st)
+                                   : run_strided<double, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st); },
                    w * N + cw * Nh, "gather+inverse dim2");
         if (r) return r;
         if (g.dim == 3) {
@@ -390,7 +451,8 @@ int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_o
                        2 * cw * Nh, "forward dim3");
             if (r) return r;
         }
-        r = timeit([&] { return run_strided<double, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, ecg, st); },
+        r = timeit([&] { return so ? run_strided<double, false, IN_SPEC, OUT_SSCATTER>(op, 2, a2, (const double*)nullptr, ecg, st)
+                                   : run_strided<double, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, ecg, st); },
                    cw * Nh + 3 * w * N, "forward dim2+scatter+CG");
         if (r) return r;
     }

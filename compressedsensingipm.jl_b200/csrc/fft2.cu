@@ -38,6 +38,9 @@ CSIPM_INST_S2(true, IN_SPEC, OUT_SPEC, EpiStore<double>)
 CSIPM_INST_S2(false, IN_SPEC, OUT_SPEC, EpiStore<double>)
 CSIPM_INST_S2(false, IN_SPEC, OUT_SCATTER, EpiStore<double>)
 CSIPM_INST_S2(false, IN_SPEC, OUT_SCATTER, EpiCG<double>)
+CSIPM_INST_S2(true, IN_SGATHER, OUT_SPEC, EpiStore<double>)
+CSIPM_INST_S2(false, IN_SPEC, OUT_SSCATTER, EpiStore<double>)
+CSIPM_INST_S2(false, IN_SPEC, OUT_SSCATTER, EpiCG<double>)
 #undef CSIPM_INST_S2
 
 template cudaError_t launch_row2<double, IN_SPEC, OUT_SPEC, true>(int, int, const PassArgs<double>&, cudaStream_t);

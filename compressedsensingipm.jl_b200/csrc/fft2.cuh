@@ -58,8 +58,21 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
             const int x = t + B * q;
             if (!live) {
                 v[q] = zero;
-            } else if (IN == IN_SPEC) {
+            } else if constexpr (IN == IN_SPEC) {
                 v[q] = a.spec[base + (long long)x * a.sx];
+            } else if constexpr (IN == IN_SGATHER) {
+                int j, k;
+                jk_of(a.jk_mode, o, x, j, k);
+                if (interior) {
+                    const cplx_t<TS> w = reinterpret_cast<const cplx_t<TS>*>(src)[sol_pair(a.g, ii, j, k)];
+                    const T r = (T)0.7071067811865476;
+                    v[q] = mk((T)w.x * r, (T)w.y * r);
+                } else {
+                    MapEntry en = decode(a.g, ii, j, k);
+                    en.re = (int)sol_tail(a.g, en.re);
+                    if (en.kind != KIND_VERT) en.im = (int)sol_tail(a.g, en.im);
+                    v[q] = gather_val<T>(en, src);
+                }
             } else {
                 int j, k;
                 jk_of(a.jk_mode, o, x, j, k);
@@ -80,9 +93,28 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
 #pragma unroll
         for (int q = 0; q < B; ++q) u[q] = S[(s * B + q) * TB + b];
         Dft<B, INV, T>::run(u);
-        if (OUT == OUT_SPEC) {
+        if constexpr (OUT == OUT_SPEC) {
 #pragma unroll
             for (int kb = 0; kb < B; ++kb) a.spec[base + (long long)(s + A * kb) * a.sx] = u[kb];
+        } else if (OUT == OUT_SSCATTER && interior) {
+            constexpr int U = 4;
+#pragma unroll
+            for (int k0 = 0; k0 < B; k0 += U) {
+                int64_t l[U];
+                typename Epi::Pre2 pr[U];
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    if (k0 + q < B) {
+                        int j, k;
+                        jk_of(a.jk_mode, o, s + A * (k0 + q), j, k);
+                        l[q] = sol_pair(a.g, ii, j, k);
+                        pr[q] = ep.pre2(l[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < U; ++q)
+                    if (k0 + q < B) ep.put2(l[q], SQRT2_D * (double)u[k0 + q].x, SQRT2_D * (double)u[k0 + q].y, pr[q]);
+            }
         } else {
             constexpr int U = 2;
 #pragma unroll
@@ -95,6 +127,10 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
                         int j, k;
                         jk_of(a.jk_mode, o, s + A * (k0 + q), j, k);
                         en[q] = interior ? decode_interior(a.g, ii, j, k) : decode(a.g, ii, j, k);
+                        if (OUT == OUT_SSCATTER) {   // plane entries (i = 0 or M1) in solver order
+                            en[q].re = (int)sol_tail(a.g, en[q].re);
+                            if (en[q].kind != KIND_VERT) en[q].im = (int)sol_tail(a.g, en[q].im);
+                        }
                         if (en[q].src) {
                             pr[q] = ep.pre(en[q].re);
                             if (en[q].kind != KIND_VERT) pi[q] = ep.pre(en[q].im);
@@ -116,7 +152,7 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
             }
         }
     }
-    if (OUT == OUT_SCATTER) ep.finish();
+    if (OUT == OUT_SCATTER || OUT == OUT_SSCATTER) ep.finish();
 }
 
 // ---------------------------------------------------------------- row pass

@@ -45,6 +45,7 @@ struct Geom {
     int ld1;        // pitch of the spectrum along dim 1 (complex elements)
     int64_t N;      // n1*n2*n3
     int64_t Nh;     // (m1+1)*n2*n3
+    int64_t NI;     // (m1-1)*n2*n3: interior half-spectrum positions (solver-order pairs)
     // 3D block offsets (0-based beta index where each region starts)
     int oE2, oE1;            // j-edges, i-edges (k-edges start at 8)
     int oFi, oFj, oFk, oC;   // faces i, faces j, faces k, interior
@@ -64,6 +65,7 @@ inline Geom make_geom(int dim, const int* n, int ld1) {
     g.ld1 = ld1;
     g.N = (int64_t)g.n1 * g.n2 * g.n3;
     g.Nh = (int64_t)(g.m1 + 1) * g.n2 * g.n3;
+    g.NI = (int64_t)(g.m1 - 1) * g.n2 * g.n3;
     g.P23 = g.p2 * g.p3; g.P13 = g.p1 * g.p3; g.P12 = g.p1 * g.p2; g.P123 = g.p1 * g.p2 * g.p3;
     g.oE2 = 8 + 8 * g.p3;
     g.oE1 = g.oE2 + 8 * g.p2;
@@ -227,6 +229,38 @@ CSIPM_HD MapEntry decode_interior(const Geom& g, int i, int j, int k) {
 
 CSIPM_HD MapEntry decode(const Geom& g, int i, int j, int k) {
     return g.dim == 3 ? decode3(g, i, j, k) : (g.dim == 2 ? decode2(g, i, j) : decode1(g, i));
+}
+
+// ---------------------------------------------------------------- solver order
+// The interior-point solve keeps its beta-space vectors in a "solver order"
+// that follows the half spectrum instead of the reference packing:
+//
+//   pairs: for 1 <= i <= M1-1 (every such position is a source of a pair),
+//          x[2q], x[2q+1] with q = (k*N2 + j)*(M1-1) + (i-1) hold
+//          sqrt2*(Re X, Im X) = (beta[re], +-beta[im]), the sign of the
+//          reference's MINUS pairs folded in;
+//   tail:  the 2*N2*N3 entries of the planes i = 0 and i = M1 (vertices,
+//          edges along j and k, faces i) in reference order, from 2*NI on.
+//
+// A gather is then one 16-byte load per spectrum position and a scatter one
+// 16-byte store, with the same (i, j, k) walk as the spectrum itself.  The map
+// is a signed permutation; the LASSO objective, the split-variable bounds and
+// every step of the interior-point method commute with it, so the solve in
+// solver order follows the same iterates (up to the order of floating-point
+// sums) and its result is mapped back to reference order at the end.
+CSIPM_HD int64_t sol_pair(const Geom& g, int i, int j, int k) {
+    return ((int64_t)k * g.n2 + j) * (g.m1 - 1) + (i - 1);
+}
+
+// solver-order index of a plane entry (reference index `ref`, i = 0 or M1)
+CSIPM_HD int64_t sol_tail(const Geom& g, int ref) {
+    const int64_t t = (g.dim == 3 && ref >= g.oFi) ? (int64_t)ref - g.oFi + g.oE1 : (int64_t)ref;
+    return 2 * g.NI + t;
+}
+
+// reference index of tail entry t (0 <= t < 2*N2*N3)
+CSIPM_HD int64_t sol_tail_ref(const Geom& g, int64_t t) {
+    return (g.dim == 3 && t >= g.oE1) ? t - g.oE1 + g.oFi : t;
 }
 
 }  // namespace csipm

@@ -86,6 +86,8 @@ struct csipm_handle_s {
 
     // model / IPM vectors (FP64)
     double* b = nullptr;            // A^T z0
+    bool sorder = false;            // solve runs in solver order (geometry.h)
+    double* bs = nullptr;           // A^T z0 in solver order (when sorder)
     double *beta = nullptr, *c = nullptr, *z1 = nullptr, *z2 = nullptr, *Qb = nullptr, *rd = nullptr;
     double *Db = nullptr, *Minv = nullptr, *rhs = nullptr, *dba = nullptr, *db = nullptr;
     double *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr;
@@ -156,7 +158,11 @@ cudaError_t run_strided(FftOperator<T>& op, int axis, const PassArgs<T>& a, cons
         const int A = axis == 3 ? op.s3_A : op.s2_A, B = axis == 3 ? op.s3_B : op.s2_B;
         if (A) return launch_strided2<T, INV, IN, OUT, TS, Epi>(A, B, a, src, epi, st);
     }
-    return launch_strided<T, INV, IN, OUT>(axis == 3 ? op.s3_cfg : op.s2_cfg, a, src, epi, st);
+    if constexpr (IN == IN_SGATHER || OUT == OUT_SSCATTER) {
+        return cudaErrorInvalidValue;   // solver order runs on the two-level kernels only
+    } else {
+        return launch_strided<T, INV, IN, OUT>(axis == 3 ? op.s3_cfg : op.s2_cfg, a, src, epi, st);
+    }
 }
 
 // Row pass: the two-level kernel for 2D/3D spectrum/real passes with an
@@ -170,8 +176,18 @@ cudaError_t run_row(FftOperator<T>& op, const PassArgs<T>& a, const TS* src, con
     return launch_row<T, IN, OUT, MASK>(op.row_cfg, a, src, epi, st);
 }
 
+// True when beta-space vectors of the solve can be kept in solver order
+// (geometry.h): the gather and scatter passes along dim 2 then run on the
+// two-level kernels.
+template <typename T>
+inline bool solver_order_ok(const FftOperator<T>& op) {
+    return std::is_same<T, double>::value && op.g.dim >= 2 && op.s2_A != 0;
+}
+
 // ------------------------------------------------------------------ operator
-template <typename T, typename TS, class Epi>
+// SOL: x and the epilogue's beta-space operands are in solver order
+// (requires solver_order_ok(op)).
+template <typename T, typename TS, class Epi, bool SOL = false>
 cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* skip, cudaStream_t st) {
     const Geom& g = op.g;
     const double sc = 1.0 / (2.0 * (double)g.N);
@@ -180,26 +196,30 @@ cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* s
     cudaError_t e;
     PassArgs<T> ra = op.row_args(sc, nullptr, nullptr);
     ra.skip = skip;
-    if (g.dim == 1) {
+    constexpr int GIN = SOL ? IN_SGATHER : IN_GATHER;
+    constexpr int SOUT = SOL ? OUT_SSCATTER : OUT_SCATTER;
+    if constexpr (SOL) {
+        if (!solver_order_ok(op)) return cudaErrorInvalidValue;
+    } else if (g.dim == 1) {
         return mask ? run_row<T, IN_GATHER, OUT_SCATTER, true>(op, ra, x, epi, st)
                     : run_row<T, IN_GATHER, OUT_SCATTER, false>(op, ra, x, epi, st);
     }
     if (g.dim == 2) {
         PassArgs<T> a2 = op.strided_args(2);
         a2.skip = skip;
-        e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st);
+        e = run_strided<T, true, GIN, OUT_SPEC>(op, 2, a2, x, none, st);
         if (e != cudaSuccess) return e;
         e = mask ? run_row<T, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
                  : run_row<T, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st);
         if (e != cudaSuccess) return e;
-        return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, epi, st);
+        return run_strided<T, false, IN_SPEC, SOUT>(op, 2, a2, (const double*)nullptr, epi, st);
     }
     // 3D: the beta-side passes run along dim 2 (line stride N1/2+1 elements),
     // the plain spectrum passes along dim 3 (stride (N1/2+1)*N2)
     PassArgs<T> a3 = op.strided_args(3), a2 = op.strided_args(2);
     a3.skip = skip;
     a2.skip = skip;
-    e = run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st);
+    e = run_strided<T, true, GIN, OUT_SPEC>(op, 2, a2, x, none, st);
     if (e != cudaSuccess) return e;
     e = run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
@@ -208,7 +228,7 @@ cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* s
     if (e != cudaSuccess) return e;
     e = run_strided<T, false, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
-    return run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, epi, st);
+    return run_strided<T, false, IN_SPEC, SOUT>(op, 2, a2, (const double*)nullptr, epi, st);
 }
 
 // x = P(sqrt(N) Re ifft(B beta))
@@ -260,6 +280,17 @@ inline int read_slots(csipm_handle h, int first, int count) {
     return CSIPM_OK;
 }
 
+
+// A^T A for the solve's vectors (solver order when the handle uses it)
+template <class Epi>
+cudaError_t solve_AtA(csipm_handle h, const double* x, const Epi& epi, const int* skip, cudaStream_t st) {
+    return h->sorder ? op_AtA<double, double, Epi, true>(h->op64, x, epi, skip, st)
+                     : op_AtA<double, double, Epi, false>(h->op64, x, epi, skip, st);
+}
+
+// signed permutation reference order <-> solver order (n = N entries)
+cudaError_t to_solver_order(const Geom& g, const double* ref, double* sol, cudaStream_t st);
+cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cudaStream_t st);
 
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
 int ensure_kkt_buffers(csipm_handle h);

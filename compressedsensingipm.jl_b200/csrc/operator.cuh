@@ -34,8 +34,9 @@
 
 namespace csipm {
 
-enum PassIn { IN_SPEC = 0, IN_GATHER = 1, IN_REAL = 2 };
-enum PassOut { OUT_SPEC = 0, OUT_SCATTER = 1, OUT_REAL = 2 };
+// *_SGATHER / *_SSCATTER: beta-space vectors in solver order (geometry.h)
+enum PassIn { IN_SPEC = 0, IN_GATHER = 1, IN_REAL = 2, IN_SGATHER = 3 };
+enum PassOut { OUT_SPEC = 0, OUT_SCATTER = 1, OUT_REAL = 2, OUT_SSCATTER = 3 };
 
 constexpr double SQRT2_D = 1.4142135623730951;
 
@@ -85,12 +86,19 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 // loop can issue the loads of several elements before it consumes them.
 struct NoPre {};
 
+// pre2 / put2 act on the solver-order pair l (elements 2l, 2l+1) with one
+// vector access per operand.
 template <typename TO>
 struct EpiStore {
     TO* out;
     using Pre = NoPre;
+    using Pre2 = NoPre;
     __device__ __forceinline__ NoPre pre(int) const { return {}; }
     __device__ __forceinline__ void put(int l, double v, const NoPre&) { out[l] = (TO)v; }
+    __device__ __forceinline__ NoPre pre2(int64_t) const { return {}; }
+    __device__ __forceinline__ void put2(int64_t l, double x, double y, const NoPre&) {
+        reinterpret_cast<cplx_t<TO>*>(out)[l] = mk((TO)x, (TO)y);
+    }
     __device__ __forceinline__ void finish() {}
 };
 
@@ -103,11 +111,21 @@ struct EpiCG {
     RedWorkspace ws;
     double acc;
     struct Pre { double p, d; };
+    struct Pre2 { cplx_t<TV> p, d; };
     __device__ __forceinline__ Pre pre(int l) const { return Pre{(double)p[l], (double)D[l]}; }
     __device__ __forceinline__ void put(int l, double v, const Pre& r) {
         const TV qv = (TV)(v + r.d * r.p);
         q[l] = qv;
         acc += r.p * (double)qv;
+    }
+    __device__ __forceinline__ Pre2 pre2(int64_t l) const {
+        return Pre2{reinterpret_cast<const cplx_t<TV>*>(p)[l], reinterpret_cast<const cplx_t<TV>*>(D)[l]};
+    }
+    __device__ __forceinline__ void put2(int64_t l, double x, double y, const Pre2& r) {
+        const TV qx = (TV)(x + (double)r.d.x * (double)r.p.x);
+        const TV qy = (TV)(y + (double)r.d.y * (double)r.p.y);
+        reinterpret_cast<cplx_t<TV>*>(q)[l] = mk(qx, qy);
+        acc += (double)r.p.x * (double)qx + (double)r.p.y * (double)qy;
     }
     __device__ __forceinline__ void finish() {
         double a[1] = {acc};

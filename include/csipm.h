@@ -85,6 +85,10 @@ typedef struct {
     int ir_max;                /* mixed precision: max FP64 refinement steps per Newton solve */
     int verbose;               /* 1: print one line per IPM iteration to stderr */
     void* stream;              /* cudaStream_t every call of the handle runs on; NULL: the default stream */
+    int layout;                /* csipm_solve's internal vector order: 0 (default) the half-spectrum
+                                  "solver order" where the operator supports it (2D/3D), 1 the
+                                  reference packing throughout.  Inputs and outputs of every entry
+                                  point are in the reference packing either way. */
 } csipm_options;
 
 /* Per-solve statistics (MadNLPExecutionStats analogue + the reference's timers,

@@ -38,7 +38,8 @@ def _problem(kind, dims, seed):
 
 
 @pytest.mark.parametrize("kind,dims", [("1d", (2048,)), ("1d", (16384,)), ("2d", (64, 64)), ("2d", (128, 96)),
-                                       ("3d", (16, 16, 16)), ("3d", (32, 32, 32))])
+                                       ("2d", (96, 128)), ("3d", (16, 16, 16)), ("3d", (32, 32, 32)),
+                                       ("3d", (32, 64, 24)), ("3d", (64, 64, 64))])
 def test_parity_with_cpu_twin(cuda, kind, dims):
     """Same seed, same algorithm: beta within 1e-6 relative, objective within
     1e-8 relative, IPM iteration count within 1."""
@@ -61,3 +62,26 @@ def test_parity_with_cpu_twin(cuda, kind, dims):
     assert abs(Fg - Fc) <= 1e-8 * Fc
     assert abs(res.stats["ipm_iter"] - info["ipm_iter"]) <= 1
     assert abs(res.stats["obj"] - info["obj"]) <= 1e-8 * abs(info["obj"])
+
+
+@pytest.mark.parametrize("kind,dims", [("2d", (64, 64)), ("2d", (200, 160)), ("3d", (32, 64, 24)),
+                                       ("3d", (40, 128, 32)), ("3d", (64, 64, 64))])
+def test_solver_order_matches_reference_order(cuda, kind, dims):
+    """The solve in the half-spectrum solver order (second dimension with a
+    two-level factor pair: 64, 128, 160, 256, 320) and in the reference packing
+    take the same iterates up to the order of floating-point sums."""
+    import csipm
+    torch = cuda
+    prob = _problem(kind, dims, seed=3)
+    size = prob.size
+    out = {}
+    for layout in ("solver", "reference"):
+        params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+        nlp = csipm.FFTNLPModel(params, rdft=True, tol=1e-10, layout=layout)
+        res = csipm.ipm_solve(nlp)
+        assert res.status == 0, res.stats
+        out[layout] = res
+    bs, br = out["solver"].beta.cpu().numpy(), out["reference"].beta.cpu().numpy()
+    assert np.linalg.norm(bs - br) / np.linalg.norm(br) <= 1e-7
+    assert abs(out["solver"].stats["ipm_iter"] - out["reference"].stats["ipm_iter"]) <= 1
+    assert abs(out["solver"].stats["lasso_obj"] - out["reference"].stats["lasso_obj"]) <= 1e-10 * abs(out["reference"].stats["lasso_obj"])
