@@ -39,6 +39,9 @@ WORKLOADS = {
     "1d16384": dict(kind="1d", dims=(16384,)),
 }
 METRIC = "s-to-solve 3D 320^3 (beta 1e-6 vs FP64)"
+ORACLE_TOL, ORACLE_CG_RTOL = 1e-12, 1e-10     # the FP64 accuracy oracle
+TIGHT_TOL, TIGHT_CG_RTOL = 1e-11, 1e-8        # FP64 with tight (reference-like) Newton solves
+IPM_VEC_PER_ITER = 4                           # CPU estimate: IPM elementwise work per iteration, in CG-update units
 
 
 def parse():
@@ -48,7 +51,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="3d320", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="mixed (the headline): FP32 CG products with FP64 residuals/refinement; "
+                         "the FP64 solve of the same problem is timed beside it as the accuracy oracle")
+    ap.add_argument("--tol", type=float, default=1e-10, help="IPM stop (relative duality gap / scaled KKT error)")
+    ap.add_argument("--cg-rtol", type=float, default=1e-2,
+                    help="relative tolerance of each Newton solve (inexact Newton; the library default is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     return ap.parse_args()
@@ -63,7 +71,8 @@ def workload_config(args, wl):
         "missing": {"3d": "balls r=3 on a period-16 lattice", "2d": "disks r=4 period 32 + 5% random",
                     "1d": "20 random gaps, 15%"}[wl["kind"]],
         "lambda": {"3d": "0.05*||A^T y||_inf", "2d": "0.1*||A^T y||_inf", "1d": "0.1*||A^T y||_inf"}[wl["kind"]],
-        "stop": "relative LASSO duality gap 1e-8 (or scaled KKT error 1e-8)",
+        "stop": f"relative LASSO duality gap {args.tol:g} (or scaled KKT error {args.tol:g})",
+        "newton_cg_rtol": args.cg_rtol,
         "l2": "no flush needed: the solve streams a multi-GB working set (> 126 MB L2) every CG iteration",
         "parallelism": f"replicas x{args.gpus}",
     }
@@ -210,37 +219,74 @@ def run_ours(args):
     # resident problem
     z0_dev = torch.tensor(z0_host, device="cuda")
     params = csipm.FFTParameters(len(spec.size), spec.size, z0_dev, lam, missing)
-    nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision)
+    kw = dict(tol=args.tol)
+    if args.cg_rtol is not None:
+        kw["ipm_cg_rtol"] = args.cg_rtol
+    nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision, **kw)
     stream = torch.cuda.current_stream()
     sol = torch.empty(2 * N, dtype=torch.float64, device="cuda")
     st = _native.Stats()
-
-    def solve():
-        s = L.csipm_solve(nlp.handle, ctypes.c_void_p(sol.data_ptr()), ctypes.c_void_p(sol.data_ptr() + 8 * N),
-                          ctypes.byref(st))
-        if s != 0:
-            _native.check(s, nlp.handle)
-        return st.as_dict()
-
-    for _ in range(args.warmup):
-        solve()
-    stats = []
-    clocks = ClockSampler(local)
-    D.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        stats.append(solve())
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    D.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    ms = D.max(ms)
-    last = stats[-1]
+
+    def solve(model):
+        s = L.csipm_solve(model.handle, ctypes.c_void_p(sol.data_ptr()), ctypes.c_void_p(sol.data_ptr() + 8 * N),
+                          ctypes.byref(st))
+        if s != 0:
+            _native.check(s, model.handle)
+        return st.as_dict()
+
+    def timed(model, steps, warmup, sample_clocks):
+        for _ in range(warmup):
+            solve(model)
+        stats = []
+        clocks = ClockSampler(local) if sample_clocks else None
+        D.barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        e0.record(stream)
+        for _ in range(steps):
+            stats.append(solve(model))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        D.barrier()
+        return D.max(e0.elapsed_time(e1) / steps), stats[-1], clk
+
+    ms, last, clk = timed(nlp, args.steps, args.warmup, True)
+    beta_main = sol[:N].clone()
+
+    # ---- accuracy oracle: a tight FP64 device solve of the same problem
+    # (untimed), and the FP64 path timed beside the headline solve at the
+    # same settings and with the reference's tight Newton solves
+    def rel(a, b_):
+        return float(torch.linalg.vector_norm(a - b_) / torch.linalg.vector_norm(b_))
+
+    oracle_kw = dict(tol=ORACLE_TOL, ipm_cg_rtol=ORACLE_CG_RTOL)
+    nlp_o = csipm.FFTNLPModel(params, rdft=True, precision="fp64", **oracle_kw)
+    last_o = solve(nlp_o)
+    beta_o = sol[:N].clone()
+    nlp_o.op_fft.close()
+    accuracy = {
+        "oracle": f"FP64 device solve, tol {ORACLE_TOL:g}, Newton rtol {ORACLE_CG_RTOL:g}",
+        "beta_rel_err": rel(beta_main, beta_o),
+        "lasso_obj_rel_err": abs(last["lasso_obj"] - last_o["lasso_obj"]) / abs(last_o["lasso_obj"]),
+        "ipm_iter": last["ipm_iter"], "ipm_iter_oracle": last_o["ipm_iter"],
+    }
+    accuracy["within_1e-6"] = accuracy["beta_rel_err"] <= 1e-6
+    fp64 = None
+    if args.precision == "mixed":
+        fp64 = {}
+        for name, kw64 in (("same_settings", kw), ("tight_newton", dict(tol=TIGHT_TOL, ipm_cg_rtol=TIGHT_CG_RTOL))):
+            nlp64 = csipm.FFTNLPModel(params, rdft=True, precision="fp64", **kw64)
+            ms64, last64, _ = timed(nlp64, args.steps, args.warmup, False)
+            fp64[name] = {"value": round(ms64 / 1000.0, 5), "tol": kw64["tol"],
+                          "newton_cg_rtol": kw64.get("ipm_cg_rtol", 1e-8), "ipm_iter": last64["ipm_iter"],
+                          "cg_iter": last64["cg_iter"], "matvecs": last64["matvecs"],
+                          "beta_rel_err": rel(sol[:N], beta_o), "speedup_mixed_vs_this": round(ms64 / ms, 3)}
+            nlp64.op_fft.close()
+    del beta_main, beta_o
 
     # ---- end to end through the C ABI with host buffers (pinned), per step:
     # H2D z0, csipm_create (mask from host indices, plans, A^T z0), csipm_solve,
@@ -261,7 +307,7 @@ def run_ours(args):
         prob.z0 = z0_e2e.data_ptr()
         prob.host_missing = miss.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
         prob.n_missing = int(miss.size)
-        opt = csipm._options(rdft=True, precision=args.precision)
+        opt = csipm._options(rdft=True, precision=args.precision, **kw)
         h = ctypes.c_void_p()
         _native.check(L.csipm_create(ctypes.byref(prob), ctypes.byref(opt), ctypes.byref(h)))
         s2 = _native.Stats()
@@ -332,8 +378,11 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(8 * N),
                 "includes": "H2D z0 + csipm_create (mask, plans, A^T z0) + csipm_solve + D2H beta + destroy"},
         "solve": {"ipm_iter": last["ipm_iter"], "cg_iter": last["cg_iter"], "matvecs": last["matvecs"],
-                  "gap": last["gap"], "obj": last["obj"], "status": last["status"]},
+                  "refinements": last["refinements"], "fallbacks": last["fallbacks"], "gap": last["gap"], "obj": last["obj"],
+                  "status": last["status"]},
         "roofline": roofline,
+        "accuracy": accuracy,
+        "fp64": fp64,
         "gpu_launches": launches,
         "clocks": clk,
     }
@@ -375,12 +424,12 @@ def _cpu_sample(size, keep, z0, lam, reps):
 
 def cpu_baseline(spec, z0, lam, stats):
     t_mv, t_vec, cores = _cpu_sample(spec.size, spec.keep, z0, lam, reps=2)
-    est = stats["matvecs"] * t_mv + stats["cg_iter"] * t_vec
+    est = stats["matvecs"] * t_mv + (stats["cg_iter"] + IPM_VEC_PER_ITER * stats["ipm_iter"]) * t_vec
     return {"value": round(est, 2), "unit": "s", "cores": cores, "kind": "port",
             "sample": (f"oracle FP64 (numpy + scipy.fft pocketfft, workers={cores}) on the full grid: 2 A^T A "
                        f"products ({t_mv:.2f} s each) and 2 CG vector updates ({t_vec:.2f} s each), scaled by "
-                       f"this solve's {stats['matvecs']} products and {stats['cg_iter']} CG iterations "
-                       f"(the CPU twin runs the same iteration counts)")}
+                       f"this solve's {stats['matvecs']} products, {stats['cg_iter']} CG iterations and "
+                       f"{IPM_VEC_PER_ITER} vector-update equivalents per IPM iteration ({stats['ipm_iter']})")}
 
 
 def run_reference(args):
@@ -401,7 +450,8 @@ def run_reference(args):
     sop = O.Operator(sspec.size, sspec.keep, True, workers=cores)
     sb = sop.At(sprob.z0)
     sop.n_matvec = 0
-    _, _, info = OI.ipm(sop, sb, sprob.lam, float(sprob.z0 @ sprob.z0), tol=1e-8)
+    # the reference's Newton solves are tight (Krylov atol 1e-12, rtol 0): CG rtol 1e-8 here
+    _, _, info = OI.ipm(sop, sb, sprob.lam, float(sprob.z0 @ sprob.z0), tol=args.tol, cg_rtol=1e-8)
     counts = {"matvecs": sop.n_matvec, "cg_iter": info["cg_iter"], "ipm_iter": info["ipm_iter"]}
     spec = P.make_spec(wl["kind"], dims=wl["dims"], seed=0)
     opf = O.Operator(spec.size, None, True, workers=cores)
@@ -410,7 +460,7 @@ def run_reference(args):
     for s in range(args.warmup + args.steps):
         t_mv, t_vec, _ = _cpu_sample(spec.size, spec.keep, prob.z0, prob.lam, reps=1)
         if s >= args.warmup:
-            vals.append(counts["matvecs"] * t_mv + counts["cg_iter"] * t_vec)
+            vals.append(counts["matvecs"] * t_mv + (counts["cg_iter"] + IPM_VEC_PER_ITER * counts["ipm_iter"]) * t_vec)
     v = float(np.mean(vals))
     sample = (f"CPU FP64 port of the path (numpy + scipy.fft pocketfft, workers={cores}); per step one A^T A "
               f"product and one CG vector update timed on the full {'x'.join(map(str, wl['dims']))} grid, scaled by "

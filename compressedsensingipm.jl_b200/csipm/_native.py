@@ -80,6 +80,7 @@ class Stats(ctypes.Structure):
         ("dual_inf", ctypes.c_double),
         ("solve_ms", ctypes.c_double),
         ("launches", ctypes.c_longlong),
+        ("fallbacks", ctypes.c_int),
     ]
 
     def as_dict(self):

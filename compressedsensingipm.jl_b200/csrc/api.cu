@@ -108,6 +108,190 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
 }
 
 
+// ------------------------------------------------------------------ mixed precision
+// FP32 PCG corrections on FP64 residuals (iterative refinement of the
+// condensed system).  Round 0 solves K d = rhs (or the FP64 residual of the
+// warm start x0) in FP32; each later round recomputes r = rhs - K x with the
+// FP64 operator and solves K d = r in FP32, asking only for the reduction
+// still missing (rtol * |r0| / |r|, floored at MIXED_INNER_RTOL, the level
+// FP32 products support).  When the requested rtol is itself at or above the
+// floor, round 0 alone answers it (its warm-start residual then comes from
+// the FP32 product when rtol >= MIXED_FP32_WARM_RTOL).  An FP32 round stops after
+// MIXED_ROUND_MAXIT iterations (stagnation) and the refinement goes on; an
+// FP32 breakdown (p.q <= 0 from rounding on a nearly singular direction)
+// keeps the partial correction and finishes the solve with FP64 PCG.
+constexpr double MIXED_INNER_RTOL = 1e-6;
+constexpr double MIXED_FP32_WARM_RTOL = 1e-4;
+constexpr int MIXED_ROUND_MAXIT = 100;
+
+int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
+    const long long n = h->N;
+    const int nb = ew_blocks(n);
+    cudaStream_t st = h->stream;
+    const bool pc = h->opt.preconditioner != 0;
+    const double* Minv = pc ? h->Minv : nullptr;
+    const float* Minv32 = pc ? h->f_Minv : nullptr;
+    const int ppp = passes_per_product(h->g);
+    int total = 0;
+    double r0 = -1.0, rn = -1.0;
+    // loose Newton tolerances take the warm-start residual from the FP32
+    // product: its rounding (~1e-7 relative) is far below what they ask
+    const bool fp32_warm = has_x0 && rtol >= MIXED_FP32_WARM_RTOL;
+    if (!has_x0) CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    for (int round = 0;; ++round) {
+        const double* res = rhs;
+        double rin = std::max(rtol, MIXED_INNER_RTOL);
+        if (round > 0 || (has_x0 && !fp32_warm)) {
+            EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
+            CK(solve_AtA(h, x, ep, nullptr, st));
+            resid64_kernel<<<nb, EW_THREADS, 0, st>>>(n, rhs, h->cg_q, Minv, h->cg_r, h->ws(h->slots + SL_DOT));
+            CK(cudaGetLastError());
+            h->matvecs++;
+            h->launches += ppp + 1;
+            int r = read_slots(h, SL_DOT, 1);
+            if (r) return r;
+            rn = std::sqrt(h->hslots[SL_DOT]);
+            if (!std::isfinite(rn)) return fail(h, CSIPM_ERR_NONFINITE, "non-finite refinement residual");
+            if (round == 0) {
+                r0 = rn;
+            } else {
+                if (rn <= rtol * r0) break;
+                if (round > h->opt.ir_max) break;
+                h->refinements++;
+                rin = std::min(0.5, std::max(MIXED_INNER_RTOL, rtol * r0 / rn));
+            }
+            res = h->cg_r;
+        }
+        // FP32 PCG from d = 0 on K d = res
+        CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
+        CK(cudaMemsetAsync(h->f_x, 0, sizeof(float) * n, st));
+        if (round == 0 && fp32_warm) {
+            // warm-start residual rhs - K x0 with the FP32 product (x0 rounded to FP32)
+            convert_kernel<double, float><<<nb, EW_THREADS, 0, st>>>(n, x, h->f_p);
+            EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(h->slots + SL_DUMMY), 0.0};
+            CK(solve_AtA32(h, h->f_p, ep, nullptr, st));
+            h->matvecs++;
+            h->launches += ppp + 1;
+            cg_init_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, rhs, h->f_q, 1, Minv32, h->f_r, h->f_p,
+                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
+        } else {
+            cg_init_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, res, (const float*)nullptr, 0, Minv32, h->f_r, h->f_p,
+                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
+        }
+        CK(cudaGetLastError());
+        h->launches += 1;
+        const int cap = std::min(maxit, MIXED_ROUND_MAXIT);
+        int chunk = 2, since = 0;
+        for (int it = 0; it < cap; ++it) {
+            EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
+            CK(solve_AtA32(h, h->f_p, ep, &h->cgs->done, st));
+            cg_update_kernel<float, float><<<nb, EW_THREADS, 0, st>>>(n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
+                                                                     h->ws(h->slots + SL_DUMMY), h->cgs);
+            cg_pupdate_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, it, h->f_r, Minv32, h->f_p, h->cgs);
+            CK(cudaGetLastError());
+            h->launches += ppp + 2;
+            if (++since >= chunk || it + 1 == cap) {
+                since = 0;
+                if (chunk < 8) chunk *= 2;
+                CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (h->hcgs->done) break;
+            }
+        }
+        CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        h->matvecs += h->hcgs->iters;
+        total += h->hcgs->iters;
+        if (r0 < 0.0) r0 = rn = std::sqrt(h->hcgs->rz0);   // |rhs| in the M-norm
+        add_f32_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->f_x, x);
+        CK(cudaGetLastError());
+        h->launches += 1;
+        if (h->hcgs->breakdown) {
+            int its = 0;
+            const int r = schur_cg(h, rhs, x, true, std::min(0.5, rtol * r0 / rn), maxit, &its);
+            total += its;
+            h->fallbacks++;
+            *iters = total;
+            return r;
+        }
+        if (rtol >= MIXED_INNER_RTOL && round == 0 && h->hcgs->done) break;
+    }
+    *iters = total;
+    return CSIPM_OK;
+}
+
+// Times each pass of one A^T A product (the CG product: gather -> ... ->
+// scatter with the CG epilogue) `reps` times; bytes are the algorithmic
+// bytes of the pass (beta-space reals of sizeof(T), spectrum complex of
+// 2*sizeof(T), the mask as bits).
+template <typename T>
+int profile_impl(csipm_handle h, FftOperator<T>& op, const T* x, T* D, T* q, int reps, double* ms_out,
+                 double* bytes_out, const char** names, int* npass) {
+    const Geom& g = h->g;
+    cudaStream_t st = h->stream;
+    const double N = (double)g.N, Nh = (double)g.Nh;
+    const double w = sizeof(T), cw = 2.0 * sizeof(T), maskb = op.maskw ? N / 8.0 : 0.0;
+    const bool f32 = sizeof(T) == 4;
+    EpiStore<double> none{nullptr};
+    EpiCG<T> ecg{x, D, q, h->ws(h->slots + SL_DUMMY), 0.0};
+    const bool mask = op.maskw != nullptr;
+    PassArgs<T> ra = op.row_args(1.0 / (2.0 * N), nullptr, nullptr);
+    int np = 0;
+    auto timeit = [&](auto&& launch, double bytes, const char* name) -> int {
+        CK(launch());   // warm
+        CK(cudaEventRecord(h->ev0, st));
+        for (int r = 0; r < reps; ++r) CK(launch());
+        CK(cudaEventRecord(h->ev1, st));
+        CK(cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        ms_out[np] = ms / reps;
+        bytes_out[np] = bytes;
+        names[np] = name;
+        ++np;
+        return CSIPM_OK;
+    };
+    int r = 0;
+    if (g.dim == 1) {
+        r = timeit([&] { return mask ? run_row<T, IN_GATHER, OUT_SCATTER, true>(op, ra, x, ecg, st)
+                                     : run_row<T, IN_GATHER, OUT_SCATTER, false>(op, ra, x, ecg, st); },
+                   4 * w * N + maskb, f32 ? "fp32 row: gather+FFT+scatter+CG" : "row: gather+C2R+mask+R2C+scatter+CG");
+        if (r) return r;
+    } else {
+        // the product's order: beta-side passes along dim 2 (solver-order
+        // gather/scatter when the handle uses it), plain ones along dim 3
+        PassArgs<T> a2 = op.strided_args(2);
+        const bool so = h->sorder;
+        if (so && !aligned16(x)) return fail(h, CSIPM_ERR_INVALID, "x must be 16-byte aligned");
+        r = timeit([&] { return so ? run_strided<T, true, IN_SGATHER, OUT_SPEC>(op, 2, a2, x, none, st)
+                                   : run_strided<T, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st); },
+                   w * N + cw * Nh, f32 ? "fp32 gather+inverse dim2" : "gather+inverse dim2");
+        if (r) return r;
+        if (g.dim == 3) {
+            PassArgs<T> a3 = op.strided_args(3);
+            r = timeit([&] { return run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
+                       2 * cw * Nh, f32 ? "fp32 inverse dim3" : "inverse dim3");
+            if (r) return r;
+        }
+        r = timeit([&] { return mask ? run_row<T, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
+                                     : run_row<T, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st); },
+                   2 * cw * Nh + maskb, f32 ? "fp32 row: C2R+mask+R2C dim1" : "row: C2R+mask+R2C dim1");
+        if (r) return r;
+        if (g.dim == 3) {
+            PassArgs<T> a3 = op.strided_args(3);
+            r = timeit([&] { return run_strided<T, false, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
+                       2 * cw * Nh, f32 ? "fp32 forward dim3" : "forward dim3");
+            if (r) return r;
+        }
+        r = timeit([&] { return so ? run_strided<T, false, IN_SPEC, OUT_SSCATTER>(op, 2, a2, (const double*)nullptr, ecg, st)
+                                   : run_strided<T, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, ecg, st); },
+                   cw * Nh + 3 * w * N, f32 ? "fp32 forward dim2+scatter+CG" : "forward dim2+scatter+CG");
+        if (r) return r;
+    }
+    *npass = np;
+    return CSIPM_OK;
+}
+
 }  // namespace csipm_internal
 
 extern "C" {
@@ -147,9 +331,9 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(h, CSIPM_ERR_NO_DEVICE, "no CUDA device");
     h = new csipm_handle_s();
     if (opt_in) h->opt = *opt_in; else csipm_default_options(&h->opt);
-    if (h->opt.precision != CSIPM_FP64) {
+    if (h->opt.precision != CSIPM_FP64 && h->opt.precision != CSIPM_MIXED) {
         delete h;
-        return fail(nullptr, CSIPM_ERR_UNSUPPORTED, "only CSIPM_FP64 is available in this build");
+        return fail(nullptr, CSIPM_ERR_INVALID, "precision must be CSIPM_FP64 or CSIPM_MIXED");
     }
     cudaGetDevice(&h->device);
     int n[3] = {prob->size[0], prob->dim >= 2 ? prob->size[1] : 1, prob->dim >= 3 ? prob->size[2] : 1};
@@ -175,6 +359,12 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     if (!h->op64.init(h->g, keep.empty() ? nullptr : keep.data(), h->stream, &err))
         return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
     h->bytes += h->op64.bytes;
+    const bool mixed = h->opt.precision == CSIPM_MIXED;
+    if (mixed) {
+        if (!h->op32.init(h->g, keep.empty() ? nullptr : keep.data(), h->stream, &err))
+            return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
+        h->bytes += h->op32.bytes;
+    }
     // reduction workspace: enough partials for the largest grid
     size_t maxblocks = 8192;
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * (h->g.dim == 3 ? h->g.n3 : 1));
@@ -185,9 +375,13 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     const size_t n_ = (size_t)h->N;
     if (!h->alloc(&h->partials, maxblocks * 8) || !h->alloc(&h->ticket, 1) || !h->alloc(&h->slots, SL_COUNT) ||
         !h->alloc(&h->cgs, 1) || !h->alloc(&h->b, n_) || !h->alloc(&h->beta, n_) || !h->alloc(&h->c, n_) ||
+        !h->alloc(&h->s1, n_) || !h->alloc(&h->s2, n_) ||
         !h->alloc(&h->z1, n_) || !h->alloc(&h->z2, n_) || !h->alloc(&h->Qb, n_) || !h->alloc(&h->rd, n_) ||
         !h->alloc(&h->Db, n_) || !h->alloc(&h->Minv, n_) || !h->alloc(&h->rhs, n_) || !h->alloc(&h->dba, n_) ||
         !h->alloc(&h->db, n_) || !h->alloc(&h->cg_r, n_) || !h->alloc(&h->cg_p, n_) || !h->alloc(&h->cg_q, n_))
+        return bail(CSIPM_ERR_OOM, h->err);
+    if (mixed && (!h->alloc(&h->f_Db, n_) || !h->alloc(&h->f_Minv, n_) || !h->alloc(&h->f_r, n_) ||
+                  !h->alloc(&h->f_p, n_) || !h->alloc(&h->f_q, n_) || !h->alloc(&h->f_x, n_)))
         return bail(CSIPM_ERR_OOM, h->err);
     if (cudaMallocHost(&h->hslots, sizeof(double) * SL_COUNT) != cudaSuccess ||
         cudaMallocHost(&h->hcgs, sizeof(CgScalars)) != cudaSuccess)
@@ -209,7 +403,7 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         cudaStreamSynchronize(h->stream) != cudaSuccess)
         return bail(CSIPM_ERR_CUDA, "synchronisation failed after A^T z0");
     h->z0sq = h->hslots[SL_DOT];
-    if (h->opt.layout == 0 && solver_order_ok(h->op64)) {
+    if (h->opt.layout == 0 && solver_order_ok(h->op64) && (!mixed || solver_order_ok(h->op32))) {
         if (!h->alloc(&h->bs, n_)) return bail(CSIPM_ERR_OOM, h->err);
         if (to_solver_order(h->g, h->b, h->bs, h->stream) != cudaSuccess ||
             cudaStreamSynchronize(h->stream) != cudaSuccess)
@@ -272,7 +466,10 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     const csipm_options& o = h->opt;
     csipm_stats S{};
     const int mv0 = h->matvecs;
+    const int rf0 = h->refinements;
+    const int fb0 = h->fallbacks;
     const long long la0 = h->launches;
+    const bool mixed = o.precision == CSIPM_MIXED;
     const int ppp = passes_per_product(h->g);
     cudaEventRecord(h->ev0, st);
     // every beta-space vector of the solve is in solver order when h->sorder
@@ -286,7 +483,8 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         h->matvecs++;
     }
     h->launches += 2 + ppp;
-    ipm_init2_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->c, h->z1, h->z2);
+    ipm_init2_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->s1, h->s2, h->z1,
+                                                 h->z2);
     CK(cudaGetLastError());
     {
         int r0 = read_slots(h, SL_MAXB, 2);
@@ -303,9 +501,11 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
             h->matvecs++;
             h->launches += ppp;
         }
-        h->launches += 1;   // residual
-        ipm_residual_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->c, h->z1, h->z2, h->rd,
-                                                       h->ws(h->slots + SL_RED));
+        h->launches += 1;   // residual + barrier diagonals + predictor right-hand side
+        ipm_resdiag_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
+                                                             h->rd, h->Db, h->Minv, mixed ? h->f_Db : nullptr,
+                                                             mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
+                                                             h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
         int r = read_slots(h, SL_RED, RR_N);
         if (r) return r;
@@ -330,16 +530,13 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
                          R[RR_RDINF], R[RR_RCINF], F, S.cg_iter);
         if (gap <= o.tol || kkt <= o.tol) { status = CSIPM_OK; break; }
         if (k >= o.max_iter) { status = CSIPM_ERR_IPM_MAXITER; break; }
-        ipm_diag_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, h->beta, h->c, h->z1, h->z2, h->Db, h->Minv,
-                                                           (double*)nullptr, (double*)nullptr, o.preconditioner);
-        // ---- predictor (affine scaling)
-        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->c, h->z1, h->z2, h->rd, nullptr, 0.0, h->rhs);
-        CK(cudaGetLastError());
+        // ---- predictor (affine scaling): diagonals and right-hand side came with the residual
         int its = 0;
-        int cs = schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
+        int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its)
+                       : schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->c, h->z1, h->z2, nullptr, 0.0, h->dba,
+        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, 0.0, h->dba,
                                                         h->ws(h->slots + SL_SS));
         CK(cudaGetLastError());
         r = read_slots(h, SL_SS, SS_N);
@@ -350,12 +547,13 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         const double sigma = std::pow(std::max(mu_aff, 0.0) / mu, 3.0);
         const double sigmu = sigma * mu;
         // ---- corrector
-        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->c, h->z1, h->z2, h->rd, h->dba, sigmu, h->rhs);
+        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba, sigmu, h->rhs);
         CK(cudaMemcpyAsync(h->db, h->dba, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        cs = schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its);
+        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its)
+                   : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->c, h->z1, h->z2, h->dba, sigmu, h->db,
+        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu, h->db,
                                                         h->ws(h->slots + SL_SS));
         CK(cudaGetLastError());
         r = read_slots(h, SL_SS, SS_N);
@@ -364,9 +562,15 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         const double ap = std::min(1.0, eta * Q[SS_MINP]);
         const double ad = std::min(1.0, eta * Q[SS_MIND]);
         a = std::min(ap, ad);
-        ipm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->c, h->z1, h->z2, h->dba, sigmu, h->db, a, a);
+        ipm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu, h->db,
+                                                      a, a);
         CK(cudaGetLastError());
-        h->launches += 7;   // diag, 2 rhs, 2 step statistics, update (+ CG launches counted in schur_cg)
+        h->launches += 4;   // corrector rhs, 2 step statistics, update (+ CG launches counted in the Newton solves)
+    }
+    if (c_out) {
+        half_sum_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->s1, h->s2, h->c);
+        CK(cudaGetLastError());
+        h->launches += 1;
     }
     if (h->sorder) {
         CK(to_reference_order(h->g, h->beta, beta_out, st));
@@ -384,6 +588,8 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     S.status = status;
     S.ipm_iter = k;
     S.matvecs = h->matvecs - mv0;
+    S.refinements = h->refinements - rf0;
+    S.fallbacks = h->fallbacks - fb0;
     S.launches = h->launches - la0;
     if (stats) *stats = S;
     if (status == CSIPM_ERR_IPM_MAXITER) fail(h, status, "IPM reached max_iter before the tolerance");
@@ -393,69 +599,19 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
 int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_out, double* bytes_out,
                          char* name_out, int* npass) {
     if (!h || !x || !ms_out || !bytes_out || !npass || reps < 1) return fail(h, CSIPM_ERR_INVALID, "bad argument");
-    FftOperator<double>& op = h->op64;
-    const Geom& g = h->g;
-    cudaStream_t st = h->stream;
-    const double N = (double)g.N, Nh = (double)g.Nh;
-    const double w = 8.0, cw = 16.0, maskb = op.maskw ? N / 8.0 : 0.0;
-    CK(cudaMemsetAsync(h->Db, 0, sizeof(double) * g.N, st));
-    EpiStore<double> none{nullptr};
-    EpiCG<double> ecg{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
-    const bool mask = op.maskw != nullptr;
-    PassArgs<double> ra = op.row_args(1.0 / (2.0 * N), nullptr, nullptr);
-    int np = 0;
     const char* names[8];
-    auto timeit = [&](auto&& launch, double bytes, const char* name) -> int {
-        CK(launch());   // warm
-        CK(cudaEventRecord(h->ev0, st));
-        for (int r = 0; r < reps; ++r) CK(launch());
-        CK(cudaEventRecord(h->ev1, st));
-        CK(cudaEventSynchronize(h->ev1));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-        ms_out[np] = ms / reps;
-        bytes_out[np] = bytes;
-        names[np] = name;
-        ++np;
-        return CSIPM_OK;
-    };
-    int r = 0;
-    if (g.dim == 1) {
-        r = timeit([&] { return mask ? run_row<double, IN_GATHER, OUT_SCATTER, true>(op, ra, x, ecg, st)
-                                     : run_row<double, IN_GATHER, OUT_SCATTER, false>(op, ra, x, ecg, st); },
-                   4 * w * N + maskb, "row: gather+C2R+mask+R2C+scatter+CG");
-        if (r) return r;
+    int np = 0, r = 0;
+    if (h->opt.precision == CSIPM_MIXED) {
+        // the FP32 passes of the CG product, on x rounded to FP32
+        convert_kernel<double, float><<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, h->f_p);
+        CK(cudaGetLastError());
+        CK(cudaMemsetAsync(h->f_Db, 0, sizeof(float) * h->N, h->stream));
+        r = profile_impl<float>(h, h->op32, h->f_p, h->f_Db, h->f_q, reps, ms_out, bytes_out, names, &np);
     } else {
-        // same order as the product: beta-side passes along dim 2, plain ones along dim 3
-        PassArgs<double> a2 = op.strided_args(2);
-        // (the solve's order: solver-order gather/scatter when the handle uses it)
-        const bool so = h->sorder;
-        if (so && !aligned16(x)) return fail(h, CSIPM_ERR_INVALID, "x must be 16-byte aligned");
-        r = timeit([&] { return so ? run_strided<double, true, IN_SGATHER, OUT_SPEC>(op, 2, a2, x, none, st)
-                                   : run_strided<double, true, IN_GATHER, OUT_SPEC>(op, 2, a2, x, none, st); },
-                   w * N + cw * Nh, "gather+inverse dim2");
-        if (r) return r;
-        if (g.dim == 3) {
-            PassArgs<double> a3 = op.strided_args(3);
-            r = timeit([&] { return run_strided<double, true, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
-                       2 * cw * Nh, "inverse dim3");
-            if (r) return r;
-        }
-        r = timeit([&] { return mask ? run_row<double, IN_SPEC, OUT_SPEC, true>(op, ra, (const double*)nullptr, none, st)
-                                     : run_row<double, IN_SPEC, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st); },
-                   2 * cw * Nh + maskb, "row: C2R+mask+R2C dim1");
-        if (r) return r;
-        if (g.dim == 3) {
-            PassArgs<double> a3 = op.strided_args(3);
-            r = timeit([&] { return run_strided<double, false, IN_SPEC, OUT_SPEC>(op, 3, a3, (const double*)nullptr, none, st); },
-                       2 * cw * Nh, "forward dim3");
-            if (r) return r;
-        }
-        r = timeit([&] { return so ? run_strided<double, false, IN_SPEC, OUT_SSCATTER>(op, 2, a2, (const double*)nullptr, ecg, st)
-                                   : run_strided<double, false, IN_SPEC, OUT_SCATTER>(op, 2, a2, (const double*)nullptr, ecg, st); },
-                   cw * Nh + 3 * w * N, "forward dim2+scatter+CG");
-        if (r) return r;
+        CK(cudaMemsetAsync(h->Db, 0, sizeof(double) * h->N, h->stream));
+        r = profile_impl<double>(h, h->op64, x, h->Db, h->cg_q, reps, ms_out, bytes_out, names, &np);
     }
+    if (r) return r;
     *npass = np;
     if (name_out)
         for (int k = 0; k < np; ++k) {

@@ -6,10 +6,11 @@ namespace csipm {
 
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
 cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
-    const dim3 grid((a.n_lines + FFT2_TB - 1) / FFT2_TB, a.n_outer, 1);
+    constexpr int TB = fft2_tb<T>();
+    const dim3 grid((a.n_lines + TB - 1) / TB, a.n_outer, 1);
 #define CSIPM_S2(AA, BB)                                                                                   \
     if (A == AA && B == BB) {                                                                              \
-        strided2_kernel<T, AA, BB, INV, IN, OUT, TS, Epi><<<grid, FFT2_TB * (AA > BB ? AA : BB), 0, st>>>(a, src, epi); \
+        strided2_kernel<T, AA, BB, INV, IN, OUT, TS, Epi><<<grid, TB * (AA > BB ? AA : BB), 0, st>>>(a, src, epi); \
         return cudaGetLastError();                                                                         \
     }
     CSIPM_S2(16, 20) CSIPM_S2(16, 16) CSIPM_S2(10, 16) CSIPM_S2(8, 16) CSIPM_S2(8, 8)
@@ -31,22 +32,14 @@ cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st) {
     return cudaErrorInvalidValue;
 }
 
-#define CSIPM_INST_S2(INV, IN, OUT, EPI) \
-    template cudaError_t launch_strided2<double, INV, IN, OUT, double, EPI>(int, int, const PassArgs<double>&, const double*, const EPI&, cudaStream_t);
-CSIPM_INST_S2(true, IN_GATHER, OUT_SPEC, EpiStore<double>)
-CSIPM_INST_S2(true, IN_SPEC, OUT_SPEC, EpiStore<double>)
-CSIPM_INST_S2(false, IN_SPEC, OUT_SPEC, EpiStore<double>)
-CSIPM_INST_S2(false, IN_SPEC, OUT_SCATTER, EpiStore<double>)
-CSIPM_INST_S2(false, IN_SPEC, OUT_SCATTER, EpiCG<double>)
-CSIPM_INST_S2(true, IN_SGATHER, OUT_SPEC, EpiStore<double>)
-CSIPM_INST_S2(false, IN_SPEC, OUT_SSCATTER, EpiStore<double>)
-CSIPM_INST_S2(false, IN_SPEC, OUT_SSCATTER, EpiCG<double>)
+#define CSIPM_INST_S2(T, INV, IN, OUT, TS, EPI) \
+    template cudaError_t launch_strided2<T, INV, IN, OUT, TS, EPI>(int, int, const PassArgs<T>&, const TS*, const EPI&, cudaStream_t);
+CSIPM_FFT2_STRIDED_LIST(CSIPM_INST_S2)
 #undef CSIPM_INST_S2
 
-template cudaError_t launch_row2<double, IN_SPEC, OUT_SPEC, true>(int, int, const PassArgs<double>&, cudaStream_t);
-template cudaError_t launch_row2<double, IN_SPEC, OUT_SPEC, false>(int, int, const PassArgs<double>&, cudaStream_t);
-template cudaError_t launch_row2<double, IN_SPEC, OUT_REAL, true>(int, int, const PassArgs<double>&, cudaStream_t);
-template cudaError_t launch_row2<double, IN_SPEC, OUT_REAL, false>(int, int, const PassArgs<double>&, cudaStream_t);
-template cudaError_t launch_row2<double, IN_REAL, OUT_SPEC, false>(int, int, const PassArgs<double>&, cudaStream_t);
+#define CSIPM_INST_R2(T, IN, OUT, MASK) \
+    template cudaError_t launch_row2<T, IN, OUT, MASK>(int, int, const PassArgs<T>&, cudaStream_t);
+CSIPM_FFT2_ROW_LIST(CSIPM_INST_R2)
+#undef CSIPM_INST_R2
 
 }  // namespace csipm

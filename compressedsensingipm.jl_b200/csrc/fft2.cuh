@@ -19,7 +19,9 @@
 
 namespace csipm {
 
-constexpr int FFT2_TB = 8;      // lines per CTA of the strided two-level pass (FP64: 128 B per access)
+// lines per CTA of the strided two-level pass: 128 B per access (8 FP64 or 16 FP32 complex)
+constexpr int FFT2_TB = 8;
+template <typename T> constexpr int fft2_tb() { return sizeof(T) == 8 ? 8 : 16; }
 
 // twiddle of the strided pass: W_L^e (forward) from a table of L-th roots
 template <bool INV, typename C>
@@ -31,10 +33,10 @@ __device__ __forceinline__ C tw_apply(C v, const C* __restrict__ tw, int e) {
 
 // ------------------------------------------------------------ strided pass
 template <typename T, int A, int B, bool INV, int IN, int OUT, typename TS, class Epi>
-__global__ void __launch_bounds__(FFT2_TB * (A > B ? A : B))
+__global__ void __launch_bounds__(fft2_tb<T>() * (A > B ? A : B))
 strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
-    constexpr int TB = FFT2_TB;
+    constexpr int TB = fft2_tb<T>();
     constexpr int L = A * B;
     if (a.skip && *a.skip) return;
     __shared__ C S[L * TB];
@@ -113,7 +115,7 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
                 }
 #pragma unroll
                 for (int q = 0; q < U; ++q)
-                    if (k0 + q < B) ep.put2(l[q], SQRT2_D * (double)u[k0 + q].x, SQRT2_D * (double)u[k0 + q].y, pr[q]);
+                    if (k0 + q < B) ep.put2(l[q], (T)SQRT2_D * u[k0 + q].x, (T)SQRT2_D * u[k0 + q].y, pr[q]);
             }
         } else {
             constexpr int U = 2;
@@ -321,10 +323,45 @@ cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, c
 template <typename T, int IN, int OUT, bool MASK>
 cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st);
 
-// epilogues the two-level strided pass is instantiated with
-template <class Epi> struct Fft2Epi { static constexpr bool value = false; };
-template <> struct Fft2Epi<EpiStore<double>> { static constexpr bool value = true; };
-template <> struct Fft2Epi<EpiCG<double>> { static constexpr bool value = true; };
+// The instantiations of the two-level passes (fft2.cu): (T, INV, IN, OUT, TS,
+// Epi) and (T, IN, OUT, MASK).  Fft2S / Fft2R tell the dispatch which exist.
+#define CSIPM_FFT2_STRIDED_LIST(X)                                   \
+    X(double, true, IN_GATHER, OUT_SPEC, double, EpiStore<double>)   \
+    X(double, true, IN_SPEC, OUT_SPEC, double, EpiStore<double>)     \
+    X(double, false, IN_SPEC, OUT_SPEC, double, EpiStore<double>)    \
+    X(double, false, IN_SPEC, OUT_SCATTER, double, EpiStore<double>) \
+    X(double, false, IN_SPEC, OUT_SCATTER, double, EpiCG<double>)    \
+    X(double, true, IN_SGATHER, OUT_SPEC, double, EpiStore<double>)  \
+    X(double, false, IN_SPEC, OUT_SSCATTER, double, EpiStore<double>) \
+    X(double, false, IN_SPEC, OUT_SSCATTER, double, EpiCG<double>)   \
+    X(float, true, IN_GATHER, OUT_SPEC, float, EpiStore<double>)     \
+    X(float, true, IN_SGATHER, OUT_SPEC, float, EpiStore<double>)    \
+    X(float, true, IN_SPEC, OUT_SPEC, double, EpiStore<double>)      \
+    X(float, false, IN_SPEC, OUT_SPEC, double, EpiStore<double>)     \
+    X(float, false, IN_SPEC, OUT_SCATTER, double, EpiCG<float>)      \
+    X(float, false, IN_SPEC, OUT_SSCATTER, double, EpiCG<float>)
+
+#define CSIPM_FFT2_ROW_LIST(X)           \
+    X(double, IN_SPEC, OUT_SPEC, true)   \
+    X(double, IN_SPEC, OUT_SPEC, false)  \
+    X(double, IN_SPEC, OUT_REAL, true)   \
+    X(double, IN_SPEC, OUT_REAL, false)  \
+    X(double, IN_REAL, OUT_SPEC, false)  \
+    X(float, IN_SPEC, OUT_SPEC, true)    \
+    X(float, IN_SPEC, OUT_SPEC, false)
+
+template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
+struct Fft2S { static constexpr bool value = false; };
+template <typename T, int IN, int OUT, bool MASK>
+struct Fft2R { static constexpr bool value = false; };
+#define CSIPM_FFT2_HAS_S(T, INV, IN, OUT, TS, EPI) \
+    template <> struct Fft2S<T, INV, IN, OUT, TS, EPI> { static constexpr bool value = true; };
+#define CSIPM_FFT2_HAS_R(T, IN, OUT, MASK) \
+    template <> struct Fft2R<T, IN, OUT, MASK> { static constexpr bool value = true; };
+CSIPM_FFT2_STRIDED_LIST(CSIPM_FFT2_HAS_S)
+CSIPM_FFT2_ROW_LIST(CSIPM_FFT2_HAS_R)
+#undef CSIPM_FFT2_HAS_S
+#undef CSIPM_FFT2_HAS_R
 
 }  // namespace csipm
 
@@ -333,7 +370,7 @@ namespace csipm {
 template <typename T>
 inline void FftOperator<T>::choose_two_level() {
     s2_A = s2_B = s3_A = s3_B = r_A = r_B = 0;
-    if (sizeof(T) != 8 || g.dim < 2) return;
+    if (g.dim < 2) return;
     int A = 0, B = 0;
     if (fft2_factor(g.n2, &A, &B) && fft2_strided_pair(A, B)) { s2_A = A; s2_B = B; }
     if (g.dim == 3 && fft2_factor(g.n3, &A, &B) && fft2_strided_pair(A, B)) { s3_A = A; s3_B = B; }

@@ -72,6 +72,7 @@ struct csipm_handle_s {
     double lambda = 0.0;
     double z0sq = 0.0;
     FftOperator<double> op64;
+    FftOperator<float> op32;        // mixed precision: the CG products
     std::string err;
     size_t bytes = 0;
     std::vector<void*> allocs;
@@ -89,11 +90,16 @@ struct csipm_handle_s {
     bool sorder = false;            // solve runs in solver order (geometry.h)
     double* bs = nullptr;           // A^T z0 in solver order (when sorder)
     double *beta = nullptr, *c = nullptr, *z1 = nullptr, *z2 = nullptr, *Qb = nullptr, *rd = nullptr;
+    double *s1 = nullptr, *s2 = nullptr;    // slacks c + beta, c - beta (stored; c is output scratch)
     double *Db = nullptr, *Minv = nullptr, *rhs = nullptr, *dba = nullptr, *db = nullptr;
     double *cg_r = nullptr, *cg_p = nullptr, *cg_q = nullptr;
     // KKT plugin (allocated on first use)
     double *L1 = nullptr, *L2 = nullptr, *P11 = nullptr, *P12 = nullptr, *P22 = nullptr;
     double *k_b = nullptr, *k_x = nullptr, *k_r = nullptr, *k_p = nullptr, *k_q = nullptr;
+    // mixed precision: FP32 copies of the Schur diagonal / preconditioner and the FP32 CG vectors
+    float *f_Db = nullptr, *f_Minv = nullptr, *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_x = nullptr;
+    int refinements = 0;
+    int fallbacks = 0;              // mixed Newton solves finished in FP64 after an FP32 breakdown
 
     // counters / timers
     int matvecs = 0;
@@ -105,6 +111,7 @@ struct csipm_handle_s {
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         op64.release();
+        op32.release();
         if (hslots) cudaFreeHost(hslots);
         if (hcgs) cudaFreeHost(hcgs);
         if (ev0) cudaEventDestroy(ev0);
@@ -154,7 +161,7 @@ enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_COUN
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
 cudaError_t run_strided(FftOperator<T>& op, int axis, const PassArgs<T>& a, const TS* src, const Epi& epi,
                         cudaStream_t st) {
-    if constexpr (Fft2Epi<Epi>::value && std::is_same<T, double>::value && std::is_same<TS, double>::value) {
+    if constexpr (Fft2S<T, INV, IN, OUT, TS, Epi>::value) {
         const int A = axis == 3 ? op.s3_A : op.s2_A, B = axis == 3 ? op.s3_B : op.s2_B;
         if (A) return launch_strided2<T, INV, IN, OUT, TS, Epi>(A, B, a, src, epi, st);
     }
@@ -169,8 +176,7 @@ cudaError_t run_strided(FftOperator<T>& op, int axis, const PassArgs<T>& a, cons
 // instantiated factor pair, else the Stockham kernel (also all 1D passes).
 template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
 cudaError_t run_row(FftOperator<T>& op, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
-    if constexpr (std::is_same<T, double>::value && IN != IN_GATHER && OUT != OUT_SCATTER &&
-                  !(IN == IN_REAL && OUT == OUT_REAL) && !(IN == IN_REAL && MASK)) {
+    if constexpr (Fft2R<T, IN, OUT, MASK>::value) {
         if (op.r_A && op.g.dim >= 2) return launch_row2<T, IN, OUT, MASK>(op.r_A, op.r_B, a, st);
     }
     return launch_row<T, IN, OUT, MASK>(op.row_cfg, a, src, epi, st);
@@ -181,7 +187,7 @@ cudaError_t run_row(FftOperator<T>& op, const PassArgs<T>& a, const TS* src, con
 // two-level kernels.
 template <typename T>
 inline bool solver_order_ok(const FftOperator<T>& op) {
-    return std::is_same<T, double>::value && op.g.dim >= 2 && op.s2_A != 0;
+    return op.g.dim >= 2 && op.s2_A != 0;
 }
 
 // ------------------------------------------------------------------ operator
@@ -288,11 +294,18 @@ cudaError_t solve_AtA(csipm_handle h, const double* x, const Epi& epi, const int
                      : op_AtA<double, double, Epi, false>(h->op64, x, epi, skip, st);
 }
 
+template <class Epi>
+cudaError_t solve_AtA32(csipm_handle h, const float* x, const Epi& epi, const int* skip, cudaStream_t st) {
+    return h->sorder ? op_AtA<float, float, Epi, true>(h->op32, x, epi, skip, st)
+                     : op_AtA<float, float, Epi, false>(h->op32, x, epi, skip, st);
+}
+
 // signed permutation reference order <-> solver order (n = N entries)
 cudaError_t to_solver_order(const Geom& g, const double* ref, double* sol, cudaStream_t st);
 cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cudaStream_t st);
 
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
+int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
 int ensure_kkt_buffers(csipm_handle h);
 
 }  // namespace csipm_internal

@@ -70,6 +70,12 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
     if (sc->done) return;
     const double pq = sc->pq;
     const double rz = sc->rz[it & 1];
+    // breakdown: every block sees the same p.q and returns before touching
+    // x or r, so the iterate stays the last good one
+    if (!(pq > 0.0) || !isfinite(pq)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) { sc->breakdown = 1; sc->done = 1; sc->iters = it; }
+        return;
+    }
     const double alpha = rz / pq;
     double acc[1] = {0.0};
     CSIPM_GRID_LOOP(i, n) {
@@ -83,7 +89,7 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
         const double rzn = ws.out[0];
         sc->rz[(it + 1) & 1] = rzn;
         sc->iters = it + 1;
-        if (!(pq > 0.0) || !isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
+        if (!isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
         else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
     }
 }
@@ -98,6 +104,23 @@ static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restri
         const double zv = Minv ? (double)Minv[i] * (double)r[i] : (double)r[i];
         p[i] = (TV)(zv + b * (double)p[i]);
     }
+}
+
+// Mixed precision: r = rhs - q in FP64 with r.(Minv r) (the refinement residual)
+static __global__ void resid64_kernel(long long n, const double* __restrict__ rhs, const double* __restrict__ q,
+                                      const double* __restrict__ Minv, double* __restrict__ r, RedWorkspace ws) {
+    double acc[1] = {0.0};
+    CSIPM_GRID_LOOP(i, n) {
+        const double rv = rhs[i] - q[i];
+        r[i] = rv;
+        acc[0] += Minv ? rv * Minv[i] * rv : rv * rv;
+    }
+    grid_reduce<1>(acc, ws, 0u, 0u);
+}
+
+// x += d (FP32 correction into the FP64 iterate)
+static __global__ void add_f32_kernel(long long n, const float* __restrict__ d, double* __restrict__ x) {
+    CSIPM_GRID_LOOP(i, n) x[i] += (double)d[i];
 }
 
 // ------------------------------------------------------------------ IPM state
@@ -123,9 +146,13 @@ static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ 
 // Dual start from the clipped gradient with lz = max(lambda, 1e-3 |b|_inf, 1e-12)
 // (the floor keeps lambda = 0 interior); c = |beta| + mu0/min(z1,z2),
 // mu0 = 0.1*lz*max(1e-3, max|beta|).  mx = {max|beta|, max|b|}.
+// The slacks s1 = c + beta, s2 = c - beta are the stored variables from here
+// on (MadNLP's slack formulation): recomputing them from c and beta would
+// cancel catastrophically once a bound is nearly active.
 static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                                  const double* __restrict__ beta, const double* __restrict__ mx,
-                                 double* __restrict__ c, double* __restrict__ z1, double* __restrict__ z2) {
+                                 double* __restrict__ s1, double* __restrict__ s2, double* __restrict__ z1,
+                                 double* __restrict__ z2) {
     const double lz = fmax(fmax(lam, 1e-3 * mx[1]), 1e-12);
     const double mu0 = 0.1 * lz * fmax(1e-3, mx[0]);
     CSIPM_GRID_LOOP(i, n) {
@@ -134,19 +161,31 @@ static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ 
         const double a = 0.5 * (lz + g), d = 0.5 * (lz - g);
         z1[i] = a;
         z2[i] = d;
-        c[i] = fabs(beta[i]) + mu0 / fmin(a, d);
+        const double be = beta[i];
+        const double ce = fabs(be) + mu0 / fmin(a, d);
+        s1[i] = ce + be;
+        s2[i] = ce - be;
     }
 }
 
-// rd = Qb - b - z1 + z2 (stored) and the scalar diagnostics
-static __global__ void ipm_residual_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
-                                    const double* __restrict__ beta, const double* __restrict__ c,
-                                    const double* __restrict__ z1, const double* __restrict__ z2,
-                                    double* __restrict__ rd, RedWorkspace ws) {
+// One pass per interior-point iteration over the state: the dual residual
+// rd = Qb - b - z1 + z2 and the scalar diagnostics (reductions RR_*), the
+// barrier diagonals of the condensed Schur system Db = 4 D1 D2/(D1 + D2),
+// Minv = 1/(1 + Db) (FP32 copies for mixed precision), and the predictor
+// right-hand side (ipm_rhs_kernel with sigmu = 0 and no correction, where
+// h1 = -z1, h2 = -z2 and fc = -lambda).
+template <typename TV>
+static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb,
+                                          double lam, const double* __restrict__ beta, const double* __restrict__ s1v,
+                                          const double* __restrict__ s2v, const double* __restrict__ z1,
+                                          const double* __restrict__ z2, double* __restrict__ rd,
+                                          double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
+                                          TV* __restrict__ Minv_lo, int precond, double* __restrict__ rhs,
+                                          RedWorkspace ws) {
     double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
     CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i], q = Qb[i], bb = b[i];
-        const double s1 = ce + be, s2 = ce - be;
+        const double be = beta[i], s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i], q = Qb[i], bb = b[i];
+        const double ce = 0.5 * (s1 + s2);
         const double r = q - bb - a + d;
         rd[i] = r;
         const double rc = lam - a - d;
@@ -158,34 +197,24 @@ static __global__ void ipm_residual_kernel(long long n, const double* __restrict
         acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
         acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
         acc[RR_SUMC] += ce;
+        const double D1 = a / s1, D2 = d / s2;
+        const double L1 = D1 + D2, L2 = D1 - D2;
+        const double dbv = 4.0 * D1 * D2 / L1;
+        const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
+        Db[i] = dbv;
+        Minv[i] = mi;
+        if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
+        rhs[i] = -r - a + d + L2 * lam / L1;
     }
     grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
-}
-
-// Barrier diagonals of the condensed Schur system: Db = 4 D1 D2/(D1 + D2), Minv = 1/(1 + Db)
-template <typename TV>
-static __global__ void ipm_diag_kernel(long long n, const double* __restrict__ beta, const double* __restrict__ c,
-                                const double* __restrict__ z1, const double* __restrict__ z2,
-                                double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
-                                TV* __restrict__ Minv_lo, int precond) {
-    CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], ce = c[i];
-        const double D1 = z1[i] / (ce + be), D2 = z2[i] / (ce - be);
-        const double db = 4.0 * D1 * D2 / (D1 + D2);
-        const double mi = precond ? 1.0 / (1.0 + db) : 1.0;
-        Db[i] = db;
-        Minv[i] = mi;
-        if (Db_lo) { Db_lo[i] = (TV)db; Minv_lo[i] = (TV)mi; }
-    }
 }
 
 // Newton direction of one element given db, the centring target sigmu and the
 // second-order correction (cor1, cor2).
 struct ElemDir { double dc, ds1, ds2, dz1, dz2; };
 
-__device__ __forceinline__ ElemDir elem_direction(double be, double ce, double a, double d, double lam,
+__device__ __forceinline__ ElemDir elem_direction(double s1, double s2, double a, double d, double lam,
                                                   double sigmu, double cor1, double cor2, double db) {
-    const double s1 = ce + be, s2 = ce - be;
     const double D1 = a / s1, D2 = d / s2;
     const double L1 = D1 + D2, L2 = D1 - D2;
     const double h1 = (sigmu - s1 * a - cor1) / s1;
@@ -202,19 +231,18 @@ __device__ __forceinline__ ElemDir elem_direction(double be, double ce, double a
 }
 
 // rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 ; corrector uses the affine direction dba
-static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2,
                                const double* __restrict__ rd, const double* __restrict__ dba, double sigmu,
                                double* __restrict__ rhs) {
     CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
         double cor1 = 0.0, cor2 = 0.0;
         if (dba) {
-            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
             cor1 = f.ds1 * f.dz1;
             cor2 = f.ds2 * f.dz2;
         }
-        const double s1 = ce + be, s2 = ce - be;
         const double D1 = a / s1, D2 = d / s2;
         const double L1 = D1 + D2, L2 = D1 - D2;
         const double h1 = (sigmu - s1 * a - cor1) / s1;
@@ -229,21 +257,20 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
 enum { SS_MINP = 0, SS_MIND, SS_SZ, SS_CROSS, SS_DD, SS_N };
 constexpr unsigned SS_MINMASK = (1u << SS_MINP) | (1u << SS_MIND);
 
-static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ beta, const double* __restrict__ c,
+static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                      const double* __restrict__ z1, const double* __restrict__ z2,
                                      const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
                                      RedWorkspace ws) {
     double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
     CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
         double cor1 = 0.0, cor2 = 0.0;
         if (dba) {
-            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
             cor1 = f.ds1 * f.dz1;
             cor2 = f.ds2 * f.dz2;
         }
-        const ElemDir o = elem_direction(be, ce, a, d, lam, sigmu, cor1, cor2, db[i]);
-        const double s1 = ce + be, s2 = ce - be;
+        const ElemDir o = elem_direction(s1, s2, a, d, lam, sigmu, cor1, cor2, db[i]);
         if (o.ds1 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s1 / o.ds1);
         if (o.ds2 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s2 / o.ds2);
         if (o.dz1 < 0.0) acc[SS_MIND] = fmin(acc[SS_MIND], -a / o.dz1);
@@ -255,25 +282,33 @@ static __global__ void ipm_stepstats_kernel(long long n, double lam, const doubl
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
 }
 
-// beta += ap db ; c += ap dc ; z += ad dz
-static __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ c,
-                                  double* __restrict__ z1, double* __restrict__ z2, const double* __restrict__ dba,
-                                  double sigmu, const double* __restrict__ db, double ap, double ad) {
+// beta += ap db ; s1 += ap ds1 ; s2 += ap ds2 ; z += ad dz
+static __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ s1v,
+                                  double* __restrict__ s2v, double* __restrict__ z1, double* __restrict__ z2,
+                                  const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
+                                  double ap, double ad) {
     CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], ce = c[i], a = z1[i], d = z2[i];
+        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
         double cor1 = 0.0, cor2 = 0.0;
         if (dba) {
-            const ElemDir f = elem_direction(be, ce, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
             cor1 = f.ds1 * f.dz1;
             cor2 = f.ds2 * f.dz2;
         }
         const double dbi = db[i];
-        const ElemDir o = elem_direction(be, ce, a, d, lam, sigmu, cor1, cor2, dbi);
-        beta[i] = be + ap * dbi;
-        c[i] = ce + ap * o.dc;
+        const ElemDir o = elem_direction(s1, s2, a, d, lam, sigmu, cor1, cor2, dbi);
+        beta[i] += ap * dbi;
+        s1v[i] = s1 + ap * o.ds1;
+        s2v[i] = s2 + ap * o.ds2;
         z1[i] = a + ad * o.dz1;
         z2[i] = d + ad * o.dz2;
     }
+}
+
+// c = (s1 + s2)/2
+static __global__ void half_sum_kernel(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
+                                       double* __restrict__ c) {
+    CSIPM_GRID_LOOP(i, n) c[i] = 0.5 * (s1[i] + s2[i]);
 }
 
 // ------------------------------------------------------------------ utilities
@@ -530,7 +565,7 @@ static __global__ void kcg_update_kernel(long long n, int it, double* __restrict
         const double rzn = ws.out[0];
         sc->rz[(it + 1) & 1] = rzn;
         sc->iters = it + 1;
-        if (!(pq > 0.0) || !isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
+        if (!isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
         else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
     }
 }

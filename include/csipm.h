@@ -106,6 +106,7 @@ typedef struct {
     double dual_inf;           /* final max |A^T A b - A^T z0 - z1 + z2| */
     double solve_ms;           /* wall time of csipm_solve on the device stream */
     long long launches;        /* kernels the solve launched (including early-exit CG tails) */
+    int fallbacks;             /* mixed precision: Newton solves finished in FP64 after an FP32 CG breakdown */
 } csipm_stats;
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -255,7 +256,8 @@ CSIPM_API int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* k
  * entries: ms_out[k] = average device ms per launch, bytes_out[k] = algorithmic
  * HBM bytes per launch (each array read or written once), name_out (optional,
  * 8 x 32 chars) = kernel role.  *npass receives the pass count (1, 3 or 5 for
- * 1D/2D/3D).  x: N.  The reference keeps only host-side timers
+ * 1D/2D/3D).  x: N, 16-byte aligned.  A CSIPM_MIXED handle times the FP32
+ * passes of its CG product (x rounded to FP32).  The reference keeps only host-side timers
  * (src/fft_utils.jl:24-25); this has no counterpart there. */
 CSIPM_API int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_out, double* bytes_out,
                                    char* name_out, int* npass);

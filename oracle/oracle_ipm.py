@@ -173,9 +173,7 @@ def schur_pcg(Qmul, Db, rhs, x0, rtol, maxit, preconditioner=True):
     return x, it
 
 
-def _direction(beta, c, z1, z2, lam, sigmu, cor1, cor2, db):
-    s1 = c + beta
-    s2 = c - beta
+def _direction(s1, s2, z1, z2, lam, sigmu, cor1, cor2, db):
     D1 = z1 / s1
     D2 = z2 / s2
     L1 = D1 + D2
@@ -209,6 +207,12 @@ def ipm(op, b, lam, z0sq, tol=1e-8, max_iter=2000, cg_rtol=1e-8, cg_maxit=None, 
     z2 = 0.5 * (lz - g)
     mu0 = 0.1 * lz * max(1e-3, maxb)
     c = np.abs(beta) + mu0 / np.minimum(z1, z2)
+    # the slacks s1 = c + beta, s2 = c - beta are kept as variables of their
+    # own (MadNLP's slack formulation of the inequality constraints) and take
+    # the same steps: recomputing them from c and beta cancels catastrophically
+    # once a bound is nearly active
+    s1 = c + beta
+    s2 = c - beta
     tot_cg = 0
     status = "max_iter"
     info = {}
@@ -216,8 +220,7 @@ def ipm(op, b, lam, z0sq, tol=1e-8, max_iter=2000, cg_rtol=1e-8, cg_maxit=None, 
     while True:
         if k > 0:
             Qb = Q(beta)
-        s1 = c + beta
-        s2 = c - beta
+        c = 0.5 * (s1 + s2)
         rd = Qb - b - z1 + z2
         rc = lam - z1 - z2
         mu = (s1 @ z1 + s2 @ z2) / (2 * N)
@@ -266,7 +269,7 @@ def ipm(op, b, lam, z0sq, tol=1e-8, max_iter=2000, cg_rtol=1e-8, cg_maxit=None, 
 
         dba, it = schur_pcg(Q, Db, rhs_of(0.0, 0.0, 0.0), None, cg_rtol, cg_maxit, preconditioner)
         tot_cg += it
-        aff = _direction(beta, c, z1, z2, lam, 0.0, 0.0, 0.0, dba)
+        aff = _direction(s1, s2, z1, z2, lam, 0.0, 0.0, 0.0, dba)
         minp, mind = ratios(aff)
         a = min(1.0, min(minp, mind))
         _, ds1, ds2, dz1, dz2 = aff
@@ -280,18 +283,20 @@ def ipm(op, b, lam, z0sq, tol=1e-8, max_iter=2000, cg_rtol=1e-8, cg_maxit=None, 
         cor2 = ds2 * dz2
         db, it = schur_pcg(Q, Db, rhs_of(sigmu, cor1, cor2), dba, cg_rtol, cg_maxit, preconditioner)
         tot_cg += it
-        dirn = _direction(beta, c, z1, z2, lam, sigmu, cor1, cor2, db)
+        dirn = _direction(s1, s2, z1, z2, lam, sigmu, cor1, cor2, db)
         minp, mind = ratios(dirn)
         eta = max(0.99, 1.0 - mu)
         ap = min(1.0, eta * minp)
         ad = min(1.0, eta * mind)
         a = min(ap, ad)
-        dc, _, _, dz1, dz2 = dirn
+        _, ds1, ds2, dz1, dz2 = dirn
         beta = beta + a * db
-        c = c + a * dc
+        s1 = s1 + a * ds1
+        s2 = s2 + a * ds2
         z1 = z1 + a * dz1
         z2 = z2 + a * dz2
         k += 1
+    c = 0.5 * (s1 + s2)
     info["status"] = status
     info["cg_iter"] = tot_cg
     info["ipm_iter"] = k
