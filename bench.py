@@ -59,6 +59,9 @@ def parse():
                     help="relative tolerance of each Newton solve (inexact Newton; the library default is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--passes-only", action="store_true",
+                    help="build the handle, launch each pass of one CG product twice (csipm_profile_passes, "
+                         "reps=1), print the pass list and exit: the small command for kernel captures")
     return ap.parse_args()
 
 
@@ -172,14 +175,34 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(workload):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+def ncu_traffic(workload, precision, kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary (profiles/dram_traffic.json), scaled to this workload, or None."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         d = json.load(open(p))
-        return d.get(workload)
+        e = d.get(f"{workload}/{precision}", {}).get(kernel)
+        return None if e is None else e["bytes_per_launch"]
     except Exception:
         return None
+
+
+def profile_passes(L, nlp, N, reps):
+    """csipm_profile_passes: each pass of one CG product timed alone with CUDA events."""
+    import torch
+    from csipm import _native
+    ms_p = (ctypes.c_double * 8)()
+    by_p = (ctypes.c_double * 8)()
+    names = ctypes.create_string_buffer(8 * 32)
+    npass = ctypes.c_int()
+    xr = torch.randn(N, dtype=torch.float64, device="cuda")
+    _native.check(L.csipm_profile_passes(nlp.handle, ctypes.c_void_p(xr.data_ptr()), reps, ms_p, by_p, names,
+                                         ctypes.byref(npass)), nlp.handle)
+    passes = []
+    for k in range(npass.value):
+        nm = names.raw[32 * k:32 * k + 32].split(b"\0")[0].decode()
+        passes.append({"kernel": nm, "ms": ms_p[k], "bytes": by_p[k], "GBps": by_p[k] / ms_p[k] / 1e6})
+    return passes
 
 
 # ----------------------------------------------------------------------- problem
@@ -224,6 +247,11 @@ def run_ours(args):
         kw["ipm_cg_rtol"] = args.cg_rtol
     nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision, **kw)
     stream = torch.cuda.current_stream()
+    if args.passes_only:
+        print(json.dumps({"workload": args.workload, "precision": args.precision,
+                          "passes": profile_passes(L, nlp, N, reps=1)}), flush=True)
+        D.close()
+        return
     sol = torch.empty(2 * N, dtype=torch.float64, device="cuda")
     st = _native.Stats()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -329,17 +357,7 @@ def run_ours(args):
         e2e_ms = D.max(e0.elapsed_time(e1) / args.steps)
 
     # ---- roofline of the dominant kernel (each pass timed alone, CUDA events)
-    ms_p = (ctypes.c_double * 8)()
-    by_p = (ctypes.c_double * 8)()
-    names = ctypes.create_string_buffer(8 * 32)
-    npass = ctypes.c_int()
-    xr = torch.randn(N, dtype=torch.float64, device="cuda")
-    _native.check(L.csipm_profile_passes(nlp.handle, ctypes.c_void_p(xr.data_ptr()), 10, ms_p, by_p, names,
-                                         ctypes.byref(npass)), nlp.handle)
-    passes = []
-    for k in range(npass.value):
-        nm = names.raw[32 * k:32 * k + 32].split(b"\0")[0].decode()
-        passes.append({"kernel": nm, "ms": ms_p[k], "bytes": by_p[k], "GBps": by_p[k] / ms_p[k] / 1e6})
+    passes = profile_passes(L, nlp, N, reps=10)
     dom = max(passes, key=lambda p: p["ms"])
     peak, peak_kind = measured_peaks()
     matvec_ms = sum(p["ms"] for p in passes)
@@ -352,7 +370,7 @@ def run_ours(args):
         "peak_kind": f"{peak_kind} (burst copy, kernel timed alone)",
         "unit": "GB/s",
         "frac": round(dom["GBps"] / peak, 4),
-        "traffic": ncu_traffic(args.workload),
+        "traffic": ncu_traffic(args.workload, args.precision, dom["kernel"]),
         "algorithmic_bytes_per_launch": dom["bytes"],
         "matvec": {"ms": round(matvec_ms, 4), "GBps": round(matvec_bytes / matvec_ms / 1e6, 1),
                    "frac": round(matvec_bytes / matvec_ms / 1e6 / peak, 4)},
