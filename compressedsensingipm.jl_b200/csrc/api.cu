@@ -405,6 +405,25 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     h->z0sq = h->hslots[SL_DOT];
     if (h->opt.layout == 0 && solver_order_ok(h->op64) && (!mixed || solver_order_ok(h->op32))) {
         if (!h->alloc(&h->bs, n_)) return bail(CSIPM_ERR_OOM, h->err);
+        // plane map: the entries of the planes i = 0 and i = M1 in solver order
+        const Geom& g = h->g;
+        std::vector<int4> pm((size_t)2 * g.n2 * g.n3);
+        for (int p = 0; p < 2; ++p)
+            for (int k = 0; k < g.n3; ++k)
+                for (int j = 0; j < g.n2; ++j) {
+                    const MapEntry e = decode(g, p ? g.m1 : 0, j, k);
+                    int4 t;
+                    t.x = (int)sol_tail(g, e.re);
+                    t.y = e.kind == KIND_VERT ? -1 : (int)sol_tail(g, e.im);
+                    t.z = e.kind;
+                    t.w = e.src;
+                    pm[((size_t)p * g.n3 + k) * g.n2 + j] = t;
+                }
+        if (!h->alloc(&h->pmap, pm.size())) return bail(CSIPM_ERR_OOM, h->err);
+        if (cudaMemcpy(h->pmap, pm.data(), sizeof(int4) * pm.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(CSIPM_ERR_CUDA, "plane map upload failed");
+        h->op64.pmap = h->pmap;
+        h->op32.pmap = h->pmap;
         if (to_solver_order(h->g, h->b, h->bs, h->stream) != cudaSuccess ||
             cudaStreamSynchronize(h->stream) != cudaSuccess)
             return bail(CSIPM_ERR_CUDA, "solver-order copy of A^T z0 failed");

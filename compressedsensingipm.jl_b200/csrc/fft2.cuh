@@ -69,11 +69,9 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
                     const cplx_t<TS> w = reinterpret_cast<const cplx_t<TS>*>(src)[sol_pair(a.g, ii, j, k)];
                     const T r = (T)0.7071067811865476;
                     v[q] = mk((T)w.x * r, (T)w.y * r);
-                } else {
-                    MapEntry en = decode(a.g, ii, j, k);
-                    en.re = (int)sol_tail(a.g, en.re);
-                    if (en.kind != KIND_VERT) en.im = (int)sol_tail(a.g, en.im);
-                    v[q] = gather_val<T>(en, src);
+                } else {   // planes i = 0, M1: tabulated entries (no per-element decode)
+                    const int4 t4 = a.pmap[((ii == 0 ? 0 : 1) * a.g.n3 + k) * a.g.n2 + j];
+                    v[q] = gather_val<T>(MapEntry{t4.x, t4.y, t4.z, t4.w}, src);
                 }
             } else {
                 int j, k;
@@ -128,10 +126,11 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
                     if (k0 + q < B) {
                         int j, k;
                         jk_of(a.jk_mode, o, s + A * (k0 + q), j, k);
-                        en[q] = interior ? decode_interior(a.g, ii, j, k) : decode(a.g, ii, j, k);
-                        if (OUT == OUT_SSCATTER) {   // plane entries (i = 0 or M1) in solver order
-                            en[q].re = (int)sol_tail(a.g, en[q].re);
-                            if (en[q].kind != KIND_VERT) en[q].im = (int)sol_tail(a.g, en[q].im);
+                        if (OUT == OUT_SSCATTER) {   // planes i = 0, M1 in solver order: tabulated
+                            const int4 t4 = a.pmap[((ii == 0 ? 0 : 1) * a.g.n3 + k) * a.g.n2 + j];
+                            en[q] = MapEntry{t4.x, t4.y, t4.z, t4.w};
+                        } else {
+                            en[q] = interior ? decode_interior(a.g, ii, j, k) : decode(a.g, ii, j, k);
                         }
                         if (en[q].src) {
                             pr[q] = ep.pre(en[q].re);

@@ -89,6 +89,7 @@ struct csipm_handle_s {
     double* b = nullptr;            // A^T z0
     bool sorder = false;            // solve runs in solver order (geometry.h)
     double* bs = nullptr;           // A^T z0 in solver order (when sorder)
+    int4* pmap = nullptr;           // solver-order plane map (when sorder)
     double *beta = nullptr, *c = nullptr, *z1 = nullptr, *z2 = nullptr, *Qb = nullptr, *rd = nullptr;
     double *s1 = nullptr, *s2 = nullptr;    // slacks c + beta, c - beta (stored; c is output scratch)
     double *Db = nullptr, *Minv = nullptr, *rhs = nullptr, *dba = nullptr, *db = nullptr;

@@ -61,6 +61,7 @@ struct PassArgs {
     const T* real_in;
     T* real_out;
     const int* skip;         // when non-null and *skip != 0 the pass returns at once (converged CG)
+    const int4* pmap;        // solver order: (re, im, kind, src) of the planes i = 0, M1, index (p*N3 + k)*N2 + j
 };
 
 // ------------------------------------------------------------- async copies
@@ -610,6 +611,7 @@ public:
     int s2_A = 0, s2_B = 0, s3_A = 0, s3_B = 0, r_A = 0, r_B = 0;
     size_t bytes = 0;
     bool owns = true;               // false: buffers belong to someone else; release() frees nothing
+    const int4* pmap = nullptr;     // solver-order plane map (owned by the handle)
 
     ~FftOperator() { release(); }
 
@@ -761,6 +763,7 @@ public:
         PassArgs<T> a{};
         a.g = g;
         a.spec = spec;
+        a.pmap = pmap;
         a.n_lines = g.m1 + 1;
         if (axis == 3) {
             a.pl = plan3; a.tw = tw3; a.Ltab = g.n3; a.tw_in_smem = s3_cfg.tw_in_smem;

@@ -198,58 +198,86 @@ static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict_
         acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
         acc[RR_SUMC] += ce;
         const double D1 = a / s1, D2 = d / s2;
-        const double L1 = D1 + D2, L2 = D1 - D2;
-        const double dbv = 4.0 * D1 * D2 / L1;
+        const double iL1 = 1.0 / (D1 + D2), L2 = D1 - D2;
+        const double dbv = 4.0 * D1 * D2 * iL1;
         const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
         Db[i] = dbv;
         Minv[i] = mi;
         if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
-        rhs[i] = -r - a + d + L2 * lam / L1;
+        rhs[i] = -r - a + d + L2 * lam * iL1;
     }
     grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
 }
 
+// Per-element quantities shared by every direction of one iteration:
+// 1/s1, 1/s2, D1 = z1/s1, D2 = z2/s2, L2 = D1 - D2 and 1/L1 with L1 = D1 + D2
+// (three divisions; FP64 division is the expensive part of these kernels).
+struct ElemPre { double a, d, is1, is2, D1, D2, L2, iL1; };
+
+__device__ __forceinline__ ElemPre elem_pre(double s1, double s2, double a, double d) {
+    ElemPre e;
+    e.a = a;
+    e.d = d;
+    e.is1 = 1.0 / s1;
+    e.is2 = 1.0 / s2;
+    e.D1 = a * e.is1;
+    e.D2 = d * e.is2;
+    e.L2 = e.D1 - e.D2;
+    e.iL1 = 1.0 / (e.D1 + e.D2);
+    return e;
+}
+
 // Newton direction of one element given db, the centring target sigmu and the
-// second-order correction (cor1, cor2).
+// second-order correction (cor1, cor2):
+//   h1 = (sigmu - s1 z1 - cor1)/s1,  h2 likewise,  fc = -(lambda - z1 - z2) + h1 + h2,
+//   dc = (fc - L2 db)/L1,  ds1 = dc + db,  ds2 = dc - db,  dz = h - D ds.
+// The affine direction (sigmu = 0, no correction) has h1 = -z1, h2 = -z2.
 struct ElemDir { double dc, ds1, ds2, dz1, dz2; };
 
-__device__ __forceinline__ ElemDir elem_direction(double s1, double s2, double a, double d, double lam,
-                                                  double sigmu, double cor1, double cor2, double db) {
-    const double D1 = a / s1, D2 = d / s2;
-    const double L1 = D1 + D2, L2 = D1 - D2;
-    const double h1 = (sigmu - s1 * a - cor1) / s1;
-    const double h2 = (sigmu - s2 * d - cor2) / s2;
-    const double rc = lam - a - d;
-    const double fc = -rc + h1 + h2;
+__device__ __forceinline__ ElemDir elem_dir(const ElemPre& e, double lam, double sigmu, double cor1, double cor2,
+                                            double db) {
+    const double h1 = (sigmu - cor1) * e.is1 - e.a;
+    const double h2 = (sigmu - cor2) * e.is2 - e.d;
+    const double fc = -(lam - e.a - e.d) + h1 + h2;
     ElemDir o;
-    o.dc = (fc - L2 * db) / L1;
+    o.dc = (fc - e.L2 * db) * e.iL1;
     o.ds1 = o.dc + db;
     o.ds2 = o.dc - db;
-    o.dz1 = h1 - D1 * o.ds1;
-    o.dz2 = h2 - D2 * o.ds2;
+    o.dz1 = h1 - e.D1 * o.ds1;
+    o.dz2 = h2 - e.D2 * o.ds2;
     return o;
 }
 
-// rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 ; corrector uses the affine direction dba
+__device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, double db) {
+    const double fc = -lam;   // -(lambda - z1 - z2) + h1 + h2 with h = -z
+    ElemDir o;
+    o.dc = (fc - e.L2 * db) * e.iL1;
+    o.ds1 = o.dc + db;
+    o.ds2 = o.dc - db;
+    o.dz1 = -e.a - e.D1 * o.ds1;
+    o.dz2 = -e.d - e.D2 * o.ds2;
+    return o;
+}
+
+// rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 (corrector: sigmu and the
+// second-order correction of the affine direction dba)
 static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2,
                                const double* __restrict__ rd, const double* __restrict__ dba, double sigmu,
                                double* __restrict__ rhs) {
     CSIPM_GRID_LOOP(i, n) {
-        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
+        const ElemPre e = elem_pre(s1v[i], s2v[i], z1[i], z2[i]);
         double cor1 = 0.0, cor2 = 0.0;
         if (dba) {
-            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
+            const ElemDir f = elem_affine(e, lam, dba[i]);
             cor1 = f.ds1 * f.dz1;
             cor2 = f.ds2 * f.dz2;
         }
-        const double D1 = a / s1, D2 = d / s2;
-        const double L1 = D1 + D2, L2 = D1 - D2;
-        const double h1 = (sigmu - s1 * a - cor1) / s1;
-        const double h2 = (sigmu - s2 * d - cor2) / s2;
+        const double h1 = (sigmu - cor1) * e.is1 - e.a;
+        const double h2 = (sigmu - cor2) * e.is2 - e.d;
         const double fb = -rd[i] + h1 - h2;
-        const double fc = -(lam - a - d) + h1 + h2;
-        rhs[i] = fb - L2 * fc / L1;
+        const double fc = -(lam - e.a - e.d) + h1 + h2;
+        rhs[i] = fb - e.L2 * fc * e.iL1;
     }
 }
 
@@ -257,28 +285,42 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
 enum { SS_MINP = 0, SS_MIND, SS_SZ, SS_CROSS, SS_DD, SS_N };
 constexpr unsigned SS_MINMASK = (1u << SS_MINP) | (1u << SS_MIND);
 
+// Running minimum of v/w (v >= 0, w > 0) kept as a fraction num/den, compared
+// by cross-multiplication: one division per thread instead of one per element.
+struct MinRatio {
+    double num = 1.0, den = 0.0;   // 1/0: +infinity
+    __device__ __forceinline__ void add(double v, double w) {
+        if (v * den < num * w) { num = v; den = w; }
+    }
+    __device__ __forceinline__ double value() const { return den > 0.0 ? num / den : DBL_MAX; }
+};
+
 static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                      const double* __restrict__ z1, const double* __restrict__ z2,
                                      const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
                                      RedWorkspace ws) {
     double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
+    MinRatio mp, md;
     CSIPM_GRID_LOOP(i, n) {
         const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
-        double cor1 = 0.0, cor2 = 0.0;
+        const ElemPre e = elem_pre(s1, s2, a, d);
+        ElemDir o;
         if (dba) {
-            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
-            cor1 = f.ds1 * f.dz1;
-            cor2 = f.ds2 * f.dz2;
+            const ElemDir f = elem_affine(e, lam, dba[i]);
+            o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, db[i]);
+        } else {
+            o = elem_affine(e, lam, db[i]);
         }
-        const ElemDir o = elem_direction(s1, s2, a, d, lam, sigmu, cor1, cor2, db[i]);
-        if (o.ds1 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s1 / o.ds1);
-        if (o.ds2 < 0.0) acc[SS_MINP] = fmin(acc[SS_MINP], -s2 / o.ds2);
-        if (o.dz1 < 0.0) acc[SS_MIND] = fmin(acc[SS_MIND], -a / o.dz1);
-        if (o.dz2 < 0.0) acc[SS_MIND] = fmin(acc[SS_MIND], -d / o.dz2);
+        if (o.ds1 < 0.0) mp.add(s1, -o.ds1);
+        if (o.ds2 < 0.0) mp.add(s2, -o.ds2);
+        if (o.dz1 < 0.0) md.add(a, -o.dz1);
+        if (o.dz2 < 0.0) md.add(d, -o.dz2);
         acc[SS_SZ] += s1 * a + s2 * d;
         acc[SS_CROSS] += s1 * o.dz1 + o.ds1 * a + s2 * o.dz2 + o.ds2 * d;
         acc[SS_DD] += o.ds1 * o.dz1 + o.ds2 * o.dz2;
     }
+    acc[SS_MINP] = mp.value();
+    acc[SS_MIND] = md.value();
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
 }
 
@@ -289,14 +331,15 @@ static __global__ void ipm_update_kernel(long long n, double lam, double* __rest
                                   double ap, double ad) {
     CSIPM_GRID_LOOP(i, n) {
         const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
-        double cor1 = 0.0, cor2 = 0.0;
-        if (dba) {
-            const ElemDir f = elem_direction(s1, s2, a, d, lam, 0.0, 0.0, 0.0, dba[i]);
-            cor1 = f.ds1 * f.dz1;
-            cor2 = f.ds2 * f.dz2;
-        }
+        const ElemPre e = elem_pre(s1, s2, a, d);
         const double dbi = db[i];
-        const ElemDir o = elem_direction(s1, s2, a, d, lam, sigmu, cor1, cor2, dbi);
+        ElemDir o;
+        if (dba) {
+            const ElemDir f = elem_affine(e, lam, dba[i]);
+            o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, dbi);
+        } else {
+            o = elem_affine(e, lam, dbi);
+        }
         beta[i] += ap * dbi;
         s1v[i] = s1 + ap * o.ds1;
         s2v[i] = s2 + ap * o.ds2;
