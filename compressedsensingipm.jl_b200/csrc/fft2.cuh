@@ -55,6 +55,37 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     // ---- step 1: thread t < B owns x = t + B*a
     if (t < B) {
         C v[A];
+        if constexpr (IN == IN_SGATHER) {
+            // interior lines: one base pair index plus q times a fixed stride
+            // (the branch is per thread and outside the element loop, so the
+            // A loads issue back to back)
+            if (live && interior) {
+                const cplx_t<TS>* __restrict__ s2 = reinterpret_cast<const cplx_t<TS>*>(src);
+                int j0, k0;
+                jk_of(a.jk_mode, o, t, j0, k0);
+                const int64_t p0 = sol_pair(a.g, ii, j0, k0);
+                const int64_t ps = (a.jk_mode == 0 ? (int64_t)a.g.n2 : (int64_t)1) * (a.g.m1 - 1) * B;
+                const T r = (T)0.7071067811865476;
+#pragma unroll
+                for (int q = 0; q < A; ++q) {
+                    const cplx_t<TS> w = s2[p0 + q * ps];
+                    v[q] = mk((T)w.x * r, (T)w.y * r);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < A; ++q) {
+                    const int x = t + B * q;
+                    int j, k;
+                    jk_of(a.jk_mode, o, x, j, k);
+                    if (live) {
+                        const int4 t4 = a.pmap[((ii == 0 ? 0 : 1) * a.g.n3 + k) * a.g.n2 + j];
+                        v[q] = gather_val<T>(MapEntry{t4.x, t4.y, t4.z, t4.w}, src);
+                    } else {
+                        v[q] = zero;
+                    }
+                }
+            }
+        } else {
 #pragma unroll
         for (int q = 0; q < A; ++q) {
             const int x = t + B * q;
@@ -80,6 +111,7 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
                 v[q] = gather_val<T>(en, src);
             }
         }
+        }
         Dft<A, INV, T>::run(v);
 #pragma unroll
         for (int ka = 0; ka < A; ++ka) S[(ka * B + t) * TB + b] = tw_apply<INV>(v[ka], tw, t * ka);
@@ -98,6 +130,11 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
             for (int kb = 0; kb < B; ++kb) a.spec[base + (long long)(s + A * kb) * a.sx] = u[kb];
         } else if (OUT == OUT_SSCATTER && interior) {
             constexpr int U = 4;
+            // pair index of x = s + A*kb: one base plus kb times a fixed stride
+            int j0, k0s;
+            jk_of(a.jk_mode, o, s, j0, k0s);
+            const int64_t p0 = sol_pair(a.g, ii, j0, k0s);
+            const int64_t ps = (a.jk_mode == 0 ? (int64_t)a.g.n2 : (int64_t)1) * (a.g.m1 - 1) * A;
 #pragma unroll
             for (int k0 = 0; k0 < B; k0 += U) {
                 int64_t l[U];
@@ -105,9 +142,7 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
 #pragma unroll
                 for (int q = 0; q < U; ++q) {
                     if (k0 + q < B) {
-                        int j, k;
-                        jk_of(a.jk_mode, o, s + A * (k0 + q), j, k);
-                        l[q] = sol_pair(a.g, ii, j, k);
+                        l[q] = p0 + (k0 + q) * ps;
                         pr[q] = ep.pre2(l[q]);
                     }
                 }
