@@ -59,6 +59,9 @@ def parse():
                     help="relative tolerance of each Newton solve (inexact Newton; the library default is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--serve-requests", type=int, default=160,
+                    help="requests of the serving stream measured beside the headline solve (0: skip)")
+    ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
     ap.add_argument("--passes-only", action="store_true",
                     help="build the handle, launch each pass of one CG product twice (csipm_profile_passes, "
                          "reps=1), print the pass list and exit: the small command for kernel captures")
@@ -404,11 +407,103 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if args.serve_requests > 0:
+        out["serving"] = run_serving(args, args.serve_requests, args.serve_slots, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(spec, z0_host, lam, last)
     D.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------- serving
+MAX_1D = 16384   # the longest 1D row the single-CTA row pass takes (longer rows: not yet supported)
+
+
+def serving_problems(n, seed0=1000):
+    """The serving stream's requests: seeded specs (csipm.problems.serving_spec),
+    synthesised and scaled with the library's own unmasked operator."""
+    import torch
+    import csipm
+    import csipm.problems as P
+    out = []
+    for k in range(n):
+        spec, precision = P.serving_spec(seed0 + k, max_1d=MAX_1D)
+        zeros = torch.zeros(spec.N, dtype=torch.float64, device="cuda")
+        op = csipm.FFTOperator(csipm.FFTParameters(len(spec.size), spec.size, zeros, 0.0, None))
+        x = op.M_perp_beta(torch.tensor(spec.beta_true, device="cuda")).cpu().numpy()
+        z0 = np.where(spec.keep, x + spec.noise, 0.0)
+        lam = float(spec.lam_factor * op.M_perpt_z(torch.tensor(z0, device="cuda")).abs().max().item())
+        op.close()
+        out.append(dict(size=spec.size, z0=z0, lam=lam, missing=np.flatnonzero(~spec.keep).astype(np.int64),
+                        precision=precision, kind=spec.name))
+    return out
+
+
+def run_serving(args, n_req, slots, rank):
+    """Sequential plain solves of the stream (one request at a time through the
+    C ABI from host buffers: create, solve, D2H, destroy) against the serving
+    loop: a closed run (all requests at t=0: capacity) and a Poisson run at an
+    offered rate of 5x the sequential rate (latency)."""
+    import torch
+    import csipm
+    from csipm import _native
+    from csipm.serving import Server
+    reqs = serving_problems(n_req, seed0=1000 + 100000 * rank)
+    L = csipm.lib()
+    opts = dict(tol=1e-8)
+    # sequential
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq_status = []
+    for r in reqs:
+        n = int(np.prod(r["size"]))
+        z0d = torch.tensor(r["z0"], device="cuda")
+        beta = torch.empty(n, dtype=torch.float64, device="cuda")
+        params = csipm.FFTParameters(len(r["size"]), r["size"], z0d, r["lam"], r["missing"])
+        nlp = csipm.FFTNLPModel(params, rdft=True, precision=r["precision"], **opts)
+        st = _native.Stats()
+        seq_status.append(L.csipm_solve(nlp.handle, ctypes.c_void_p(beta.data_ptr()), None, ctypes.byref(st)))
+        beta.cpu()
+        nlp.op_fft.close()
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    seq_rate = n_req / t_seq
+
+    def serve(rate):
+        rng = np.random.default_rng(7)
+        gaps = rng.exponential(1.0 / rate, size=n_req) if rate else np.zeros(n_req)
+        arrivals = np.cumsum(gaps) - gaps[0]
+        res = []
+        with Server(slots=slots) as srv:
+            t_start = time.perf_counter()
+            for k, r in enumerate(reqs):
+                while True:
+                    wait = arrivals[k] - (time.perf_counter() - t_start)
+                    if wait <= 0:
+                        break
+                    res.extend(srv.poll(timeout_ms=0))
+                    time.sleep(min(wait, 0.002))
+                srv.submit(r["size"], r["z0"], r["lam"], r["missing"], tag=k, precision=r["precision"], **opts)
+            res.extend(srv.drain())
+            t_end = time.perf_counter()
+        lat = np.array([x.latency_ms for x in res])
+        return {"solves_per_s": round(n_req / (t_end - t_start), 2),
+                "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                "failed": int(sum(x.status != 0 for x in res))}
+
+    closed = serve(0.0)
+    poisson = serve(5.0 * seq_rate)
+    kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("1d", "2d", "3d")}
+    return {
+        "requests": n_req, "slots": slots, "mix": kinds,
+        "sizes": "1D N in [2^12, %d], 2D sides in [128, 1024], 3D sides in [32, 128], log-uniform, factors 2/3/5; "
+                 "0.5-5%% sparsity; 5-20%% missing; FP64 or mixed per request; tol 1e-8" % MAX_1D,
+        "sequential_plain": {"solves_per_s": round(seq_rate, 2), "failed": int(sum(s != 0 for s in seq_status))},
+        "batched_closed": closed,
+        "batched_poisson": dict(poisson, offered_per_s=round(5.0 * seq_rate, 2)),
+        "speedup_vs_sequential": round(closed["solves_per_s"] / seq_rate, 2),
+    }
 
 
 # ----------------------------------------------------------------------- CPU baseline (oracle)

@@ -33,7 +33,8 @@ EXPORTS = (
     "csipm_get_Atz0", "csipm_beta_to_dft", "csipm_dft_to_beta", "csipm_apply_A", "csipm_apply_At",
     "csipm_apply_AtA", "csipm_obj", "csipm_grad", "csipm_cons", "csipm_hprod", "csipm_kkt_build",
     "csipm_condensed_mul", "csipm_precond_mul", "csipm_kkt_mul", "csipm_jtprod", "csipm_kkt_solve",
-    "csipm_solve", "csipm_get_timers", "csipm_profile_passes", "csipm_apply_AtA_static",
+    "csipm_solve", "csipm_get_timers", "csipm_profile_passes", "csipm_apply_AtA_static", "csipm_trim_pool",
+    "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
 )
 
 
@@ -87,6 +88,20 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("device", ctypes.c_int)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("problem", Problem), ("options", Options), ("beta_out", ctypes.c_void_p), ("tag", ctypes.c_uint64)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int), ("stats", Stats), ("queue_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_size_t)]
+
+
+
 _lib = None
 
 
@@ -129,6 +144,12 @@ def load(path: str | None = None):
         "csipm_get_timers": (I, [H, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.POINTER(dbl), I]),
         "csipm_profile_passes": (I, [H, D, I, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.c_char_p, ctypes.POINTER(I)]),
         "csipm_apply_AtA_static": (I, [I, ctypes.POINTER(I), D, D, D, ctypes.c_void_p]),
+        "csipm_trim_pool": (I, [I]),
+        "csipm_footprint": (I, [I, ctypes.POINTER(I), I, ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)]),
+        "csipm_server_create": (I, [ctypes.POINTER(ServerOptions), ctypes.POINTER(H)]),
+        "csipm_server_submit": (I, [H, ctypes.POINTER(Request)]),
+        "csipm_server_poll": (I, [H, ctypes.POINTER(Result), I, ctypes.POINTER(I), I]),
+        "csipm_server_destroy": (I, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -183,3 +183,52 @@ def known_answer_signal(size):
     b = np.cos(2 * math.pi * 2 / N2 * j) + 2 * np.sin(2 * math.pi * 2 / N2 * j)
     c = np.cos(2 * math.pi * 3 / N3 * k) + 2 * np.sin(2 * math.pi * 3 / N3 * k)
     return np.einsum("i,j,k->ijk", a, b, c).ravel(order="F")
+
+
+# ------------------------------------------------------------------ serving stream
+SERVE_RANGES = {"1d": (2 ** 12, 2 ** 20), "2d": (128, 1024), "3d": (32, 128)}
+
+
+def smooth_even(rng, lo, hi):
+    """A log-uniform draw in [lo, hi] moved to the nearest even number whose
+    prime factors are 2, 3 and 5."""
+    x = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    best = None
+    for a in range(1, 21):
+        for b in range(0, 13):
+            for c in range(0, 9):
+                v = (2 ** a) * (3 ** b) * (5 ** c)
+                if lo <= v <= hi and (best is None or abs(np.log(v / x)) < abs(np.log(best / x))):
+                    best = v
+    return best
+
+
+def serving_spec(seed, max_1d=None):
+    """One request of the serving stream: kind uniform over 1D/2D/3D; each
+    dimension log-uniform in its range (1D N in [2^12, 2^20], 2D sides in
+    [128, 1024], 3D sides in [32, 128]) with factors 2, 3, 5; sparsity
+    0.5-5% (N(0,1), log-normal with random signs in 3D); 5-20% missing (gaps
+    in 1D, a punched lattice topped up with random samples in 2D/3D);
+    sigma = 0.01; lambda factor 0.05-0.1; FP64 or mixed precision.
+    ``max_1d`` caps the 1D length."""
+    rng = np.random.default_rng(seed)
+    kind = ["1d", "2d", "3d"][rng.integers(3)]
+    lo, hi = SERVE_RANGES[kind]
+    if kind == "1d" and max_1d:
+        hi = min(hi, max_1d)
+    nd = int(kind[0])
+    size = tuple(smooth_even(rng, lo, hi) for _ in range(nd))
+    N = int(np.prod(size))
+    frac = rng.uniform(0.005, 0.05)
+    beta = _sparse_beta(rng, N, frac, lognormal=(kind == "3d"))
+    miss = rng.uniform(0.05, 0.20)
+    if kind == "1d":
+        keep = gap_mask_1d(rng, N, miss, int(rng.integers(5, 30)))
+    else:
+        keep = lattice_mask(size, 16, 3 if kind == "3d" else 2)
+        extra = max(0.0, miss - (1.0 - keep.mean()))
+        keep &= rng.random(N) >= extra
+    noise = 0.01 * rng.standard_normal(N)
+    spec = ProblemSpec(kind, size, beta, keep, noise, float(rng.uniform(0.05, 0.1)), seed)
+    precision = "mixed" if rng.random() < 0.5 else "fp64"
+    return spec, precision

@@ -12,6 +12,50 @@ namespace csipm {
 // lets every translation unit report through csipm_last_error(NULL)
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* get_last_error() { return g_last_error.c_str(); }
+
+namespace {
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+std::mutex g_pin_mu;
+std::map<size_t, std::vector<void*>> g_pinned;
+}  // namespace
+
+cudaMemPool_t device_pool(int dev) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;   // keep freed blocks for the next handle
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = pool;
+    return pool;
+}
+
+void* pinned_get(size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto& v = g_pinned[bytes];
+        if (!v.empty()) {
+            void* p = v.back();
+            v.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void pinned_put(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pinned[bytes].push_back(p);
+}
 }  // namespace csipm
 
 namespace csipm_internal {
@@ -345,26 +389,37 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     // NULL selects the CUDA default stream (the cuBLAS/cuFFT convention)
     h->stream = (cudaStream_t)h->opt.stream;
     h->own_stream = false;
-    // mask
-    std::vector<uint8_t> keep;
-    if (prob->n_missing > 0) {
+    h->pool = device_pool(h->device);
+    if (!h->pool) return bail(CSIPM_ERR_CUDA, "device memory pool creation failed");
+    h->op64.pool = h->pool;
+    h->op32.pool = h->pool;
+    // mask: indices checked here, bits built on the device from a stream-ordered copy
+    int64_t* dmiss = nullptr;
+    const int64_t nm = prob->n_missing > 0 ? prob->n_missing : 0;
+    if (nm > 0) {
         if (!prob->host_missing) return bail(CSIPM_ERR_INVALID, "host_missing is null");
-        keep.assign((size_t)h->N, 1u);
-        for (int64_t t = 0; t < prob->n_missing; ++t) {
+        for (int64_t t = 0; t < nm; ++t) {
             const int64_t idx = prob->host_missing[t];
             if (idx < 0 || idx >= h->N) return bail(CSIPM_ERR_INVALID, "missing index out of range");
-            keep[(size_t)idx] = 0u;
+        }
+        if (cudaMallocFromPoolAsync((void**)&dmiss, sizeof(int64_t) * nm, h->pool, h->stream) != cudaSuccess)
+            return bail(CSIPM_ERR_OOM, "out of device memory (missing indices)");
+        // pageable source: the call returns once the indices are staged
+        if (cudaMemcpyAsync(dmiss, prob->host_missing, sizeof(int64_t) * nm, cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess) {
+            cudaFreeAsync(dmiss, h->stream);
+            return bail(CSIPM_ERR_CUDA, "missing-index upload failed");
         }
     }
-    if (!h->op64.init(h->g, keep.empty() ? nullptr : keep.data(), h->stream, &err))
-        return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
-    h->bytes += h->op64.bytes;
     const bool mixed = h->opt.precision == CSIPM_MIXED;
-    if (mixed) {
-        if (!h->op32.init(h->g, keep.empty() ? nullptr : keep.data(), h->stream, &err))
-            return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
-        h->bytes += h->op32.bytes;
+    bool ok = h->op64.init(h->g, dmiss, nm, h->stream, &err);
+    if (ok) h->bytes += h->op64.bytes;
+    if (ok && mixed) {
+        ok = h->op32.init(h->g, dmiss, nm, h->stream, &err);
+        if (ok) h->bytes += h->op32.bytes;
     }
+    if (dmiss) cudaFreeAsync(dmiss, h->stream);
+    if (!ok) return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
     // reduction workspace: enough partials for the largest grid
     size_t maxblocks = 8192;
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * (h->g.dim == 3 ? h->g.n3 : 1));
@@ -383,9 +438,11 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     if (mixed && (!h->alloc(&h->f_Db, n_) || !h->alloc(&h->f_Minv, n_) || !h->alloc(&h->f_r, n_) ||
                   !h->alloc(&h->f_p, n_) || !h->alloc(&h->f_q, n_) || !h->alloc(&h->f_x, n_)))
         return bail(CSIPM_ERR_OOM, h->err);
-    if (cudaMallocHost(&h->hslots, sizeof(double) * SL_COUNT) != cudaSuccess ||
-        cudaMallocHost(&h->hcgs, sizeof(CgScalars)) != cudaSuccess)
-        return bail(CSIPM_ERR_OOM, "pinned host allocation failed");
+    static_assert(sizeof(double) * SL_COUNT == csipm_handle_s::HSLOT_BYTES, "slot block size");
+    static_assert(sizeof(CgScalars) <= csipm_handle_s::HCGS_BYTES, "CG scalar block size");
+    h->hslots = (double*)pinned_get(csipm_handle_s::HSLOT_BYTES);
+    h->hcgs = (CgScalars*)pinned_get(csipm_handle_s::HCGS_BYTES);
+    if (!h->hslots || !h->hcgs) return bail(CSIPM_ERR_OOM, "pinned host allocation failed");
     cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int), h->stream);
     cudaMemsetAsync(h->slots, 0, sizeof(double) * SL_COUNT, h->stream);
     cudaEventCreate(&h->ev0);
@@ -420,7 +477,8 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
                     pm[((size_t)p * g.n3 + k) * g.n2 + j] = t;
                 }
         if (!h->alloc(&h->pmap, pm.size())) return bail(CSIPM_ERR_OOM, h->err);
-        if (cudaMemcpy(h->pmap, pm.data(), sizeof(int4) * pm.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        if (cudaMemcpyAsync(h->pmap, pm.data(), sizeof(int4) * pm.size(), cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess)
             return bail(CSIPM_ERR_CUDA, "plane map upload failed");
         h->op64.pmap = h->pmap;
         h->op32.pmap = h->pmap;
@@ -430,6 +488,15 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         h->sorder = true;
     }
     *out = h;
+    return CSIPM_OK;
+}
+
+int csipm_trim_pool(int device) {
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return CSIPM_ERR_NO_DEVICE;
+    cudaMemPool_t pool = device_pool(dev);
+    if (!pool) return fail(nullptr, CSIPM_ERR_CUDA, "device memory pool unavailable");
+    if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) return fail(nullptr, CSIPM_ERR_CUDA, "cudaMemPoolTrimTo failed");
     return CSIPM_OK;
 }
 

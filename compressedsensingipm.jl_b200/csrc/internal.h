@@ -21,6 +21,17 @@
 namespace csipm {
 void set_last_error(const std::string& msg);
 const char* get_last_error();
+
+// Stream-ordered device memory for handles: one pool per device, created on
+// first use, that keeps freed blocks for the next handle (creating and
+// destroying handles then neither maps memory nor synchronises the device,
+// so handles on other streams keep running).  csipm_trim_pool releases it.
+cudaMemPool_t device_pool(int dev);
+
+// Small pinned host blocks (scalar read-back slots) from a process-wide free
+// list: cudaFreeHost would synchronise the device.
+void* pinned_get(size_t bytes);
+void pinned_put(void* p, size_t bytes);
 }  // namespace csipm
 
 namespace csipm_internal {
@@ -108,13 +119,17 @@ struct csipm_handle_s {
     double krylov_ms = 0.0, total_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
+    cudaMemPool_t pool = nullptr;   // device_pool(device): every device buffer of the handle
+    static constexpr size_t HSLOT_BYTES = sizeof(double) * 64;   // SL_COUNT slots
+    static constexpr size_t HCGS_BYTES = 64;                     // >= sizeof(CgScalars)
+
     ~csipm_handle_s() {
-        for (void* p : allocs) cudaFree(p);
+        for (void* p : allocs) cudaFreeAsync(p, stream);
         allocs.clear();
         op64.release();
         op32.release();
-        if (hslots) cudaFreeHost(hslots);
-        if (hcgs) cudaFreeHost(hcgs);
+        if (hslots) pinned_put(hslots, HSLOT_BYTES);
+        if (hcgs) pinned_put(hcgs, HCGS_BYTES);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -123,7 +138,7 @@ struct csipm_handle_s {
     template <typename P>
     bool alloc(P** p, size_t count) {
         void* q = nullptr;
-        if (cudaMalloc(&q, sizeof(P) * count) != cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&q, sizeof(P) * count, pool, stream) != cudaSuccess) {
             err = "out of device memory";
             return false;
         }

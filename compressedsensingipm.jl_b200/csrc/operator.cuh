@@ -593,6 +593,30 @@ struct PassCfg {
     dim3 grid;           // in-place path only; persistent grids are sized from occupancy at launch
 };
 
+// ------------------------------------------------------------ mask
+// Observed-sample mask, one bit per real sample, rows of N1 bits padded to
+// 32-bit words: every in-row bit set, padding clear; then the missing
+// samples' bits cleared (duplicates are harmless).
+static __global__ void mask_init_kernel(size_t words, int wpr, int n1, uint32_t* __restrict__ w) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < words; t += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(t % wpr);
+        const int nb = min(32, n1 - 32 * c);
+        w[t] = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
+    }
+}
+
+static __global__ void mask_clear_kernel(const int64_t* __restrict__ idx, int64_t n, int n1, int wpr,
+                                         uint32_t* __restrict__ w) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = idx[t];
+        const int64_t r = v / n1;
+        const int i = (int)(v - r * n1);
+        atomicAnd(&w[r * wpr + (i >> 5)], ~(1u << (i & 31)));
+    }
+}
+
+inline unsigned mask_blocks(long long n) { return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4096)); }
+
 template <typename T>
 class FftOperator {
 public:
@@ -613,24 +637,43 @@ public:
     bool owns = true;               // false: buffers belong to someone else; release() frees nothing
     const int4* pmap = nullptr;     // solver-order plane map (owned by the handle)
 
+    // stream-ordered allocations from this pool on `stream` when set (the
+    // handle's), else plain cudaMalloc/cudaFree
+    cudaMemPool_t pool = nullptr;
+
     ~FftOperator() { release(); }
+
+    template <typename P>
+    cudaError_t dalloc(P** p, size_t count) {
+        void* q = nullptr;
+        const cudaError_t e = pool ? cudaMallocFromPoolAsync(&q, sizeof(P) * count, pool, stream)
+                                   : cudaMalloc(&q, sizeof(P) * count);
+        *p = reinterpret_cast<P*>(q);
+        return e;
+    }
+    void dfree(void* p) {
+        if (!p) return;
+        if (pool) cudaFreeAsync(p, stream);
+        else cudaFree(p);
+    }
 
     void release() {
         if (!owns) return;
-        cudaFree(spec); spec = nullptr;
-        cudaFree(maskw); maskw = nullptr;
-        cudaFree(tw1); tw1 = nullptr;
-        cudaFree(tw2); tw2 = nullptr;
-        cudaFree(tw3); tw3 = nullptr;
+        dfree(spec); spec = nullptr;
+        dfree(maskw); maskw = nullptr;
+        dfree(tw1); tw1 = nullptr;
+        dfree(tw2); tw2 = nullptr;
+        dfree(tw3); tw3 = nullptr;
     }
 
-    static bool upload_table(int L, C** dst, std::string* err) {
+    bool upload_table(int L, C** dst, std::string* err) {
         std::vector<double> t;
         twiddle_table(L, &t);
         std::vector<C> h(L);
         for (int e = 0; e < L; ++e) h[e] = mk((T)t[2 * e], (T)t[2 * e + 1]);
-        if (cudaMalloc(dst, sizeof(C) * L) != cudaSuccess) { *err = "out of device memory (twiddles)"; return false; }
-        cudaMemcpy(*dst, h.data(), sizeof(C) * L, cudaMemcpyHostToDevice);
+        if (dalloc(dst, L) != cudaSuccess) { *err = "out of device memory (twiddles)"; return false; }
+        // pageable source: returns once staged, so `h` may go out of scope
+        cudaMemcpyAsync(*dst, h.data(), sizeof(C) * L, cudaMemcpyHostToDevice, stream);
         return true;
     }
 
@@ -723,7 +766,9 @@ public:
         return true;
     }
 
-    bool init(const Geom& geom, const uint8_t* host_keep, cudaStream_t st, std::string* err) {
+    // dev_missing: n_missing 0-based linear indices of missing samples in
+    // device memory (validated by the caller), or n_missing == 0 for no mask
+    bool init(const Geom& geom, const int64_t* dev_missing, int64_t n_missing, cudaStream_t st, std::string* err) {
         g = geom;
         stream = st;
         if (!make_plans(err)) return false;
@@ -736,17 +781,16 @@ public:
         if (g.dim >= 2 && !upload_table(g.n2, &tw2, err)) return false;
         if (g.dim >= 3 && !upload_table(g.n3, &tw3, err)) return false;
         const size_t spec_elems = (size_t)g.ld1 * g.n2 * g.n3;
-        if (cudaMalloc(&spec, sizeof(C) * spec_elems) != cudaSuccess) { *err = "out of device memory (spectrum)"; return false; }
+        if (dalloc(&spec, spec_elems) != cudaSuccess) { *err = "out of device memory (spectrum)"; return false; }
         bytes += sizeof(C) * spec_elems;
-        if (host_keep) {
+        if (n_missing > 0) {
             wpr = (g.n1 + 31) / 32;
-            std::vector<uint32_t> w((size_t)wpr * nrows, 0u);
-            for (int r = 0; r < nrows; ++r)
-                for (int i = 0; i < g.n1; ++i)
-                    if (host_keep[(size_t)r * g.n1 + i]) w[(size_t)r * wpr + (i >> 5)] |= 1u << (i & 31);
-            if (cudaMalloc(&maskw, sizeof(uint32_t) * w.size()) != cudaSuccess) { *err = "out of device memory (mask)"; return false; }
-            cudaMemcpy(maskw, w.data(), sizeof(uint32_t) * w.size(), cudaMemcpyHostToDevice);
-            bytes += sizeof(uint32_t) * w.size();
+            const size_t words = (size_t)wpr * nrows;
+            if (dalloc(&maskw, words) != cudaSuccess) { *err = "out of device memory (mask)"; return false; }
+            bytes += sizeof(uint32_t) * words;
+            mask_init_kernel<<<mask_blocks(words), 256, 0, stream>>>(words, wpr, g.n1, maskw);
+            mask_clear_kernel<<<mask_blocks(n_missing), 256, 0, stream>>>(dev_missing, n_missing, g.n1, wpr, maskw);
+            if (cudaGetLastError() != cudaSuccess) { *err = "mask construction failed"; return false; }
         }
         return true;
     }

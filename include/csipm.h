@@ -124,6 +124,14 @@ CSIPM_API int csipm_create(const csipm_problem* prob, const csipm_options* opt, 
 /* Frees everything the handle owns (never the caller's vectors). */
 CSIPM_API int csipm_destroy(csipm_handle h);
 
+/* Handles take their device memory from one stream-ordered pool per device
+ * that keeps freed blocks for the next handle, so csipm_create/csipm_destroy
+ * neither map memory nor synchronise the device (other handles' streams keep
+ * running).  This returns the pool's unused memory to the driver (device < 0:
+ * the current device).  No counterpart in the reference (CUDA.jl manages its
+ * own pool). */
+CSIPM_API int csipm_trim_pool(int device);
+
 /* Message of the last failure on `h` (or of the last failed csipm_create when h is NULL). */
 CSIPM_API const char* csipm_last_error(csipm_handle h);
 
@@ -247,6 +255,52 @@ CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elem
  * `stream` (NULL: default stream); errors are reported by csipm_last_error(NULL). */
 CSIPM_API int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, const double* x, double* y,
                                      void* stream);
+
+/* ---------------------------------------------------------------- serving */
+/* A request loop for many recoveries of uneven sizes (no counterpart in the
+ * reference, which solves one recovery per call, src/CompressedSensingIPM.jl:31-36).
+ * `slots` worker threads, each with its own CUDA stream, take requests in
+ * arrival order as soon as a slot is free and the request's device footprint
+ * (csipm_footprint) fits in what the admitted requests leave of `hbm_budget`;
+ * a request that does not fit yet lets smaller ones behind it go first.
+ * Admitted requests keep their interior-point state resident on the device
+ * and their kernels overlap. */
+typedef struct csipm_server_s* csipm_server;
+
+typedef struct {
+    int slots;                 /* concurrent solves; 0: 8 */
+    size_t hbm_budget;         /* device bytes admitted requests may hold; 0: 80% of the free memory at create */
+    int device;                /* CUDA device; -1: the current one */
+} csipm_server_options;
+
+typedef struct {
+    csipm_problem problem;     /* as for csipm_create, but z0 is a HOST pointer (N reals) */
+    csipm_options options;     /* from csipm_default_options, then edited; `stream` is ignored */
+    double* beta_out;          /* HOST, N reals, written before the result is posted (may be NULL) */
+    uint64_t tag;              /* the caller's id, returned with the result */
+} csipm_request;
+
+typedef struct {
+    uint64_t tag;
+    int status;                /* csipm_status of the solve */
+    csipm_stats stats;
+    double queue_ms;           /* submission -> admission */
+    double latency_ms;         /* submission -> result posted (beta_out written) */
+    size_t footprint;          /* device bytes the request was admitted with */
+} csipm_result;
+
+/* Device bytes a handle for this problem holds plus the server's staging of
+ * z0 and beta (an upper bound of csipm_get_info's figure + 16N). */
+CSIPM_API int csipm_footprint(int dim, const int* size, int precision, int64_t n_missing, size_t* bytes);
+CSIPM_API int csipm_server_create(const csipm_server_options* opt, csipm_server* out);
+/* Queues a copy of the request struct; the host buffers it points to must stay
+ * valid until its result has been polled. */
+CSIPM_API int csipm_server_submit(csipm_server s, const csipm_request* r);
+/* Moves up to `max` finished results to `out` (*n of them), waiting up to
+ * timeout_ms (-1: until one is ready or nothing is pending) when none is ready. */
+CSIPM_API int csipm_server_poll(csipm_server s, csipm_result* out, int max, int* n, int timeout_ms);
+/* Runs every queued request to completion, then frees the server. */
+CSIPM_API int csipm_server_destroy(csipm_server s);
 
 /* ---------------------------------------------------------------- diagnostics */
 

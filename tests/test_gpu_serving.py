@@ -1,0 +1,111 @@
+"""Serving loop (csipm_server_*): requests of uneven sizes admitted by device
+footprint, solved concurrently on per-slot streams.  Each result must equal the
+same request solved alone (beta within 1e-12 relative: the kernels and their
+reductions are deterministic, so concurrency changes nothing)."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MIX = [("1d", (2048,), "fp64", 1e-8), ("1d", (4096,), "mixed", 1e-2), ("2d", (64, 64), "fp64", 1e-2),
+       ("2d", (96, 128), "mixed", 1e-5), ("3d", (32, 32, 32), "fp64", 1e-8), ("3d", (32, 64, 24), "mixed", 1e-2),
+       ("3d", (48, 48, 48), "fp64", 1e-3), ("2d", (120, 64), "mixed", 1e-8), ("3d", (16, 16, 16), "mixed", 1e-4),
+       ("1d", (6000,), "fp64", 1e-3)]
+
+
+def _problem(kind, dims, seed):
+    import csipm.problems as P
+    spec = P.make_spec(kind, dims=dims, seed=seed)
+    op0 = O.Operator(spec.size)
+    return P.finalize(spec, op0.A, op0.At)
+
+
+@pytest.fixture(scope="module")
+def problems():
+    return [_problem(kind, dims, seed=10 + k) for k, (kind, dims, _, _) in enumerate(MIX)]
+
+
+def _alone(torch, prob, precision, rtol):
+    import csipm
+    size = prob.size
+    params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+    nlp = csipm.FFTNLPModel(params, rdft=True, precision=precision, tol=1e-10, ipm_cg_rtol=rtol)
+    res = csipm.ipm_solve(nlp)
+    nlp.op_fft.close()
+    return res
+
+
+def test_results_same_alone_and_in_the_mix(cuda, problems):
+    from csipm.serving import Server
+    torch = cuda
+    with Server(slots=4) as srv:
+        for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
+            srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=prec, tol=1e-10,
+                       ipm_cg_rtol=rtol)
+        got = {r.tag: r for r in srv.drain()}
+    assert sorted(got) == list(range(len(MIX)))
+    for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
+        r = got[k]
+        assert r.status == 0, (k, r.stats)
+        alone = _alone(torch, prob, prec, rtol)
+        b = alone.beta.cpu().numpy()
+        assert np.linalg.norm(r.beta - b) <= 1e-12 * np.linalg.norm(b), k
+        assert r.stats["ipm_iter"] == alone.stats["ipm_iter"]
+        assert r.latency_ms >= r.queue_ms >= 0.0
+
+
+def test_admission_by_footprint(cuda, problems):
+    """A budget that holds about one large request at a time still completes
+    every request (smaller ones go first while a large one waits)."""
+    from csipm.serving import Server, footprint
+    fps = [footprint(p.size, prec, p.missing.size if p.missing is not None else 0)
+           for p, (_, _, prec, _) in zip(problems, MIX)]
+    budget = int(1.2 * max(fps))
+    with Server(slots=4, hbm_budget=budget) as srv:
+        for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
+            srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=prec, tol=1e-10,
+                       ipm_cg_rtol=rtol)
+        res = srv.drain()
+    assert len(res) == len(MIX)
+    assert all(r.status == 0 for r in res)
+    assert all(r.footprint == fps[r.tag] for r in res)
+
+
+def test_requests_arriving_while_others_run(cuda, problems):
+    """Continuous admission: requests submitted after earlier ones are already
+    on the GPU join them; every result arrives."""
+    from csipm.serving import Server
+    with Server(slots=3) as srv:
+        half = len(MIX) // 2
+        for k in range(half):
+            prob = problems[k]
+            srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=MIX[k][2], tol=1e-10,
+                       ipm_cg_rtol=MIX[k][3])
+        first = srv.poll(timeout_ms=-1)
+        assert first
+        for k in range(half, len(MIX)):
+            prob = problems[k]
+            srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=MIX[k][2], tol=1e-10,
+                       ipm_cg_rtol=MIX[k][3])
+        rest = srv.drain()
+    tags = sorted(r.tag for r in first + rest)
+    assert tags == list(range(len(MIX)))
+    assert all(r.status == 0 for r in first + rest)
+
+
+def test_footprint_bounds_the_handle(cuda, problems):
+    """csipm_footprint is an upper bound of what a handle holds (+ the server's
+    z0/beta staging) and not far above it."""
+    import csipm
+    from csipm.serving import footprint
+    torch = cuda
+    for prob, (_, _, prec, rtol) in list(zip(problems, MIX))[:6]:
+        size = prob.size
+        params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+        nlp = csipm.FFTNLPModel(params, rdft=True, precision=prec)
+        held = nlp.op_fft.device_bytes() + 16 * int(np.prod(size))
+        fp = footprint(size, prec, prob.missing.size if prob.missing is not None else 0)
+        nlp.op_fft.close()
+        assert held <= fp <= 1.6 * held + (8 << 20), (size, held, fp)
