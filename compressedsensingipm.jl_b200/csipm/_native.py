@@ -64,6 +64,7 @@ class Options(ctypes.Structure):
         ("verbose", ctypes.c_int),
         ("stream", ctypes.c_void_p),
         ("layout", ctypes.c_int),
+        ("cuda_graphs", ctypes.c_int),
     ]
 
 

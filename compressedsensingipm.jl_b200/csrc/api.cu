@@ -102,6 +102,61 @@ cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cu
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ CG iteration loop
+// Runs PCG iterations (iteration(stream, it) launches one; `it` only selects
+// the parity of the double-buffered scalars) until the device `done` flag is
+// read back set or maxit is reached.  From the third iteration on, groups of
+// CG_GRAPH_ITERS iterations are replayed from a CUDA graph captured once per
+// handle and vector (one launch instead of CG_GRAPH_ITERS x (passes + 2));
+// iterations after convergence return at once on the device flag.  The flag
+// is read back after 2, 4, then every 8 iterations.
+constexpr int CG_GRAPH_ITERS = 4;
+
+template <class Iter>
+int cg_iterations(csipm_handle h, cudaGraphExec_t* exec, int maxit, Iter&& iteration, int per_iter) {
+    cudaStream_t st = h->stream;
+    int it = 0, chunk = 2, since = 0;
+    while (it < maxit) {
+        int step = 1;
+        if (exec && h->opt.cuda_graphs && !h->graphs_off && it >= 2 && it % 2 == 0 && it + CG_GRAPH_ITERS <= maxit) {
+            if (!*exec) {
+                cudaStream_t cs = nullptr;
+                cudaGraph_t g = nullptr;
+                bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+                          cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    for (int k = 0; k < CG_GRAPH_ITERS && ok; ++k) ok = iteration(cs, k) == cudaSuccess;
+                    ok = (cudaStreamEndCapture(cs, &g) == cudaSuccess) && ok && g;
+                }
+                if (ok) ok = cudaGraphInstantiate(exec, g, 0) == cudaSuccess;
+                if (g) cudaGraphDestroy(g);
+                if (cs) cudaStreamDestroy(cs);
+                cudaGetLastError();
+                if (!ok) {
+                    *exec = nullptr;
+                    h->graphs_off = true;   // plain launches from now on
+                }
+            }
+            if (*exec) {
+                CK(cudaGraphLaunch(*exec, st));
+                step = CG_GRAPH_ITERS;
+            }
+        }
+        if (step == 1) CK(iteration(st, it));
+        h->launches += (long long)step * per_iter;
+        it += step;
+        since += step;
+        if (since >= chunk || it >= maxit) {
+            since = 0;
+            if (chunk < 8) chunk *= 2;
+            CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (h->hcgs->done) break;
+        }
+    }
+    return CSIPM_OK;
+}
+
 // ------------------------------------------------------------------ Schur PCG
 // Solves (A'A + Db) x = rhs with preconditioner Minv (csipm_solve's inner solve).
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
@@ -123,25 +178,19 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
                                                     h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rtol);
     CK(cudaGetLastError());
     h->launches += 1;
-    int chunk = 2;
-    int it = 0;
-    int since = 0;
-    for (; it < maxit; ++it) {
+    auto iteration = [&](cudaStream_t s, int it) -> cudaError_t {
         EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
-        CK(solve_AtA(h, h->cg_p, ep, &h->cgs->done, st));
-        cg_update_kernel<double, double><<<nb, EW_THREADS, 0, st>>>(n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
-                                                                    h->ws(h->slots + SL_DUMMY), h->cgs);
-        cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, it, h->cg_r, Minv, h->cg_p, h->cgs);
-        CK(cudaGetLastError());
-        h->launches += ppp + 2;
-        if (++since >= chunk || it + 1 == maxit) {
-            since = 0;
-            if (chunk < 8) chunk *= 2;
-            CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            if (h->hcgs->done) break;
-        }
-    }
+        cudaError_t e = solve_AtA(h, h->cg_p, ep, &h->cgs->done, s);
+        if (e != cudaSuccess) return e;
+        cg_update_kernel<double, double><<<nb, EW_THREADS, 0, s>>>(n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
+                                                                   h->ws(h->slots + SL_DUMMY), h->cgs);
+        cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, s>>>(n, it, h->cg_r, Minv, h->cg_p, h->cgs);
+        return cudaGetLastError();
+    };
+    // x is a kernel argument: a graph is only valid for the vector it was captured with
+    cudaGraphExec_t* ex = x == h->dba ? &h->cg_exec64[0] : (x == h->db ? &h->cg_exec64[1] : nullptr);
+    const int r = cg_iterations(h, ex, maxit, iteration, ppp + 2);
+    if (r) return r;
     CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     h->matvecs += h->hcgs->iters;
@@ -225,22 +274,18 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         CK(cudaGetLastError());
         h->launches += 1;
         const int cap = std::min(maxit, MIXED_ROUND_MAXIT);
-        int chunk = 2, since = 0;
-        for (int it = 0; it < cap; ++it) {
+        auto iteration = [&](cudaStream_t s, int it) -> cudaError_t {
             EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
-            CK(solve_AtA32(h, h->f_p, ep, &h->cgs->done, st));
-            cg_update_kernel<float, float><<<nb, EW_THREADS, 0, st>>>(n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
-                                                                     h->ws(h->slots + SL_DUMMY), h->cgs);
-            cg_pupdate_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, it, h->f_r, Minv32, h->f_p, h->cgs);
-            CK(cudaGetLastError());
-            h->launches += ppp + 2;
-            if (++since >= chunk || it + 1 == cap) {
-                since = 0;
-                if (chunk < 8) chunk *= 2;
-                CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                if (h->hcgs->done) break;
-            }
+            cudaError_t e = solve_AtA32(h, h->f_p, ep, &h->cgs->done, s);
+            if (e != cudaSuccess) return e;
+            cg_update_kernel<float, float><<<nb, EW_THREADS, 0, s>>>(n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
+                                                                    h->ws(h->slots + SL_DUMMY), h->cgs);
+            cg_pupdate_kernel<float><<<nb, EW_THREADS, 0, s>>>(n, it, h->f_r, Minv32, h->f_p, h->cgs);
+            return cudaGetLastError();
+        };
+        {
+            const int r = cg_iterations(h, &h->cg_exec32, cap, iteration, ppp + 2);
+            if (r) return r;
         }
         CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -354,6 +399,7 @@ int csipm_default_options(csipm_options* opt) {
     opt->ipm_cg_rtol = 1e-8;
     opt->ir_max = 3;
     opt->verbose = 0;
+    opt->cuda_graphs = 1;
     opt->stream = nullptr;
     return CSIPM_OK;
 }

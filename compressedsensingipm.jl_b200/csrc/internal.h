@@ -111,6 +111,11 @@ struct csipm_handle_s {
     // mixed precision: FP32 copies of the Schur diagonal / preconditioner and the FP32 CG vectors
     float *f_Db = nullptr, *f_Minv = nullptr, *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_x = nullptr;
     int refinements = 0;
+    // CUDA graphs of CG_GRAPH_ITERS CG iterations (FP64: one per solution
+    // vector, dba and db; FP32: one), captured on first use
+    cudaGraphExec_t cg_exec64[2] = {nullptr, nullptr};
+    cudaGraphExec_t cg_exec32 = nullptr;
+    bool graphs_off = false;        // a capture failed: plain launches
     int fallbacks = 0;              // mixed Newton solves finished in FP64 after an FP32 breakdown
 
     // counters / timers
@@ -124,6 +129,9 @@ struct csipm_handle_s {
     static constexpr size_t HCGS_BYTES = 64;                     // >= sizeof(CgScalars)
 
     ~csipm_handle_s() {
+        for (auto& g : cg_exec64)
+            if (g) cudaGraphExecDestroy(g);
+        if (cg_exec32) cudaGraphExecDestroy(cg_exec32);
         for (void* p : allocs) cudaFreeAsync(p, stream);
         allocs.clear();
         op64.release();

@@ -73,7 +73,7 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
     // breakdown: every block sees the same p.q and returns before touching
     // x or r, so the iterate stays the last good one
     if (!(pq > 0.0) || !isfinite(pq)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) { sc->breakdown = 1; sc->done = 1; sc->iters = it; }
+        if (blockIdx.x == 0 && threadIdx.x == 0) { sc->breakdown = 1; sc->done = 1; }
         return;
     }
     const double alpha = rz / pq;
@@ -88,7 +88,7 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
     if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
         const double rzn = ws.out[0];
         sc->rz[(it + 1) & 1] = rzn;
-        sc->iters = it + 1;
+        sc->iters += 1;     // counted on the device: graph replays reuse the same `it` values
         if (!isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
         else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
     }
@@ -607,7 +607,7 @@ static __global__ void kcg_update_kernel(long long n, int it, double* __restrict
     if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
         const double rzn = ws.out[0];
         sc->rz[(it + 1) & 1] = rzn;
-        sc->iters = it + 1;
+        sc->iters += 1;     // counted on the device: graph replays reuse the same `it` values
         if (!isfinite(rzn)) { sc->breakdown = 1; sc->done = 1; }
         else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
     }

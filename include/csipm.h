@@ -89,6 +89,9 @@ typedef struct {
                                   "solver order" where the operator supports it (2D/3D), 1 the
                                   reference packing throughout.  Inputs and outputs of every entry
                                   point are in the reference packing either way. */
+    int cuda_graphs;           /* 1 (default): csipm_solve replays groups of CG iterations from CUDA
+                                  graphs captured once per handle; 0: plain launches (same kernels,
+                                  same results) */
 } csipm_options;
 
 /* Per-solve statistics (MadNLPExecutionStats analogue + the reference's timers,

@@ -85,3 +85,24 @@ def test_solver_order_matches_reference_order(cuda, kind, dims):
     assert np.linalg.norm(bs - br) / np.linalg.norm(br) <= 1e-7
     assert abs(out["solver"].stats["ipm_iter"] - out["reference"].stats["ipm_iter"]) <= 1
     assert abs(out["solver"].stats["lasso_obj"] - out["reference"].stats["lasso_obj"]) <= 1e-10 * abs(out["reference"].stats["lasso_obj"])
+
+
+@pytest.mark.parametrize("kind,dims,precision", [("3d", (32, 64, 24), "fp64"), ("2d", (96, 128), "mixed"),
+                                                 ("1d", (4096,), "fp64"), ("3d", (64, 64, 64), "mixed")])
+def test_cuda_graph_replay_changes_nothing(cuda, kind, dims, precision):
+    """Groups of CG iterations replayed from CUDA graphs run the same kernels
+    with the same arguments as plain launches: identical beta and counts."""
+    import csipm
+    torch = cuda
+    prob = _problem(kind, dims, seed=4)
+    size = prob.size
+    out = {}
+    for graphs in (True, False):
+        params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+        nlp = csipm.FFTNLPModel(params, rdft=True, precision=precision, tol=1e-10, cuda_graphs=graphs)
+        res = csipm.ipm_solve(nlp)
+        assert res.status == 0, res.stats
+        out[graphs] = res
+    assert torch.equal(out[True].beta, out[False].beta)
+    for key in ("ipm_iter", "cg_iter", "matvecs"):
+        assert out[True].stats[key] == out[False].stats[key]
