@@ -341,7 +341,22 @@ int profile_impl(csipm_handle h, FftOperator<T>& op, const T* x, T* D, T* q, int
         return CSIPM_OK;
     };
     int r = 0;
-    if (g.dim == 1) {
+    if (g.dim == 1 && op.l1P) {
+        const double M = (double)g.m1;
+        r = timeit([&] { return l1d_first(op, x, nullptr, st); }, 2 * w * N + cw * M,
+                   f32 ? "fp32 1D lines: gather+C2R+inverse" : "1D lines: gather+C2R+inverse");
+        if (r) return r;
+        r = timeit([&] { return mask ? l1d_row<T, IN_SPEC, OUT_SPEC, true>(op, ra.scale, nullptr, nullptr, nullptr, st)
+                                     : l1d_row<T, IN_SPEC, OUT_SPEC, false>(op, ra.scale, nullptr, nullptr, nullptr, st); },
+                   2 * cw * M + maskb, f32 ? "fp32 1D rows: inverse+mask+forward" : "1D rows: inverse+mask+forward");
+        if (r) return r;
+        r = timeit([&] { return l1d_lines_forward(op, nullptr, st); }, 2 * cw * M,
+                   f32 ? "fp32 1D lines: forward" : "1D lines: forward");
+        if (r) return r;
+        r = timeit([&] { return l1d_post(op, ecg, nullptr, st); }, 2 * cw * M + 3 * w * N,
+                   f32 ? "fp32 1D R2C+scatter+CG" : "1D R2C+scatter+CG");
+        if (r) return r;
+    } else if (g.dim == 1) {
         r = timeit([&] { return mask ? run_row<T, IN_GATHER, OUT_SCATTER, true>(op, ra, x, ecg, st)
                                      : run_row<T, IN_GATHER, OUT_SCATTER, false>(op, ra, x, ecg, st); },
                    4 * w * N + maskb, f32 ? "fp32 row: gather+FFT+scatter+CG" : "row: gather+C2R+mask+R2C+scatter+CG");

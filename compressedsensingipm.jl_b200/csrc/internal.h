@@ -16,6 +16,7 @@
 #include "fft2.cuh"
 #include "operator.cuh"
 #include "solver_kernels.cuh"
+#include "long1d.cuh"
 #include <type_traits>
 
 namespace csipm {
@@ -230,6 +231,15 @@ cudaError_t op_AtA(FftOperator<T>& op, const TS* x, const Epi& epi, const int* s
     constexpr int SOUT = SOL ? OUT_SSCATTER : OUT_SCATTER;
     if constexpr (SOL) {
         if (!solver_order_ok(op)) return cudaErrorInvalidValue;
+    } else if (g.dim == 1 && op.l1P) {
+        e = l1d_first(op, x, skip, st);
+        if (e != cudaSuccess) return e;
+        e = mask ? l1d_row<T, IN_SPEC, OUT_SPEC, true>(op, sc, nullptr, nullptr, skip, st)
+                 : l1d_row<T, IN_SPEC, OUT_SPEC, false>(op, sc, nullptr, nullptr, skip, st);
+        if (e != cudaSuccess) return e;
+        e = l1d_lines_forward(op, skip, st);
+        if (e != cudaSuccess) return e;
+        return l1d_post(op, epi, skip, st);
     } else if (g.dim == 1) {
         return mask ? run_row<T, IN_GATHER, OUT_SCATTER, true>(op, ra, x, epi, st)
                     : run_row<T, IN_GATHER, OUT_SCATTER, false>(op, ra, x, epi, st);
@@ -269,6 +279,12 @@ cudaError_t op_A(FftOperator<T>& op, const TS* beta, T* x, cudaStream_t st) {
     EpiStore<double> none{nullptr};
     PassArgs<T> ra = op.row_args(1.0 / std::sqrt((double)g.N), nullptr, x);
     cudaError_t e;
+    if (g.dim == 1 && op.l1P) {
+        e = l1d_first(op, beta, nullptr, st);
+        if (e != cudaSuccess) return e;
+        return mask ? l1d_row<T, IN_SPEC, OUT_REAL, true>(op, ra.scale, nullptr, x, nullptr, st)
+                    : l1d_row<T, IN_SPEC, OUT_REAL, false>(op, ra.scale, nullptr, x, nullptr, st);
+    }
     if (g.dim == 1)
         return mask ? run_row<T, IN_GATHER, OUT_REAL, true>(op, ra, beta, none, st)
                     : run_row<T, IN_GATHER, OUT_REAL, false>(op, ra, beta, none, st);
@@ -291,6 +307,13 @@ cudaError_t op_At(FftOperator<T>& op, const T* z, const Epi& epi, cudaStream_t s
     EpiStore<double> none{nullptr};
     PassArgs<T> ra = op.row_args(1.0 / (2.0 * std::sqrt((double)g.N)), z, nullptr);
     cudaError_t e;
+    if (g.dim == 1 && op.l1P) {
+        e = l1d_row<T, IN_REAL, OUT_SPEC, false>(op, ra.scale, z, nullptr, nullptr, st);
+        if (e != cudaSuccess) return e;
+        e = l1d_lines_forward(op, nullptr, st);
+        if (e != cudaSuccess) return e;
+        return l1d_post(op, epi, nullptr, st);
+    }
     if (g.dim == 1) return run_row<T, IN_REAL, OUT_SCATTER, false>(op, ra, (const double*)nullptr, epi, st);
     e = run_row<T, IN_REAL, OUT_SPEC, false>(op, ra, (const double*)nullptr, none, st);
     if (e != cudaSuccess) return e;
@@ -302,7 +325,9 @@ cudaError_t op_At(FftOperator<T>& op, const T* z, const Epi& epi, cudaStream_t s
 
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-inline int passes_per_product(const Geom& g) { return g.dim == 3 ? 5 : (g.dim == 2 ? 3 : 1); }
+inline int passes_per_product(const Geom& g) {
+    return g.dim == 3 ? 5 : (g.dim == 2 ? 3 : (g.m1 > L1D_MIN_M ? 4 : 1));
+}
 
 inline int read_slots(csipm_handle h, int first, int count) {
     CK(cudaMemcpyAsync(h->hslots + first, h->slots + first, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));

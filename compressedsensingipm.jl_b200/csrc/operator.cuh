@@ -617,6 +617,25 @@ static __global__ void mask_clear_kernel(const int64_t* __restrict__ idx, int64_
 
 inline unsigned mask_blocks(long long n) { return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4096)); }
 
+// Long 1D rows (long1d.cuh): rows of M above L1D_MIN_M complex values run
+// as M = P*Q over many CTAs.
+constexpr int L1D_MIN_M = 2048;
+constexpr int L1D_MAX_P = 4096;     // row length of the four-step row kernel
+constexpr int L1D_MAX_Q = 768;      // line length of the first and last passes
+constexpr int L1D_TB = 8;           // lines per CTA of the first pass
+
+// M = P*Q with Q the largest divisor of M not above sqrt(M) (nor L1D_MAX_Q),
+// P = M/Q; false when P exceeds L1D_MAX_P
+inline bool l1d_split(int M, int* P, int* Q) {
+    int best = 0;
+    for (int q = 2; (long long)q * q <= M && q <= L1D_MAX_Q; ++q)
+        if (M % q == 0) best = q;
+    if (!best || M / best > L1D_MAX_P) return false;
+    *Q = best;
+    *P = M / best;
+    return true;
+}
+
 template <typename T>
 class FftOperator {
 public:
@@ -636,6 +655,12 @@ public:
     size_t bytes = 0;
     bool owns = true;               // false: buffers belong to someone else; release() frees nothing
     const int4* pmap = nullptr;     // solver-order plane map (owned by the handle)
+    // long 1D rows: M = l1P * l1Q (0 when the one-CTA row pass is used)
+    int l1P = 0, l1Q = 0, l1RB = 0;
+    FftPlanDev planP{}, planQ{};
+    C* twP = nullptr;
+    C* twQ = nullptr;
+    PassCfg q_cfg;
 
     // stream-ordered allocations from this pool on `stream` when set (the
     // handle's), else plain cudaMalloc/cudaFree
@@ -664,6 +689,8 @@ public:
         dfree(tw1); tw1 = nullptr;
         dfree(tw2); tw2 = nullptr;
         dfree(tw3); tw3 = nullptr;
+        dfree(twP); twP = nullptr;
+        dfree(twQ); twQ = nullptr;
     }
 
     bool upload_table(int L, C** dst, std::string* err) {
@@ -771,9 +798,23 @@ public:
     bool init(const Geom& geom, const int64_t* dev_missing, int64_t n_missing, cudaStream_t st, std::string* err) {
         g = geom;
         stream = st;
-        if (!make_plans(err)) return false;
         const int nrows = g.n2 * g.n3;
-        if (!choose_row(nrows, &row_cfg, err)) return false;
+        if (g.dim == 1 && g.m1 > L1D_MIN_M) {
+            if (!l1d_split(g.m1, &l1P, &l1Q)) {
+                *err = "1D length has no split M = P*Q with P <= 4096, Q <= 768";
+                return false;
+            }
+            if (!make_fft_plan(l1P, &planP, err, max_radix()) || !make_fft_plan(l1Q, &planQ, err, max_radix()))
+                return false;
+            if (!choose_strided(planQ, l1Q, l1P, 1, &q_cfg, err)) return false;
+            l1RB = 1;
+            while (l1RB < 16 && 2 * (size_t)l1P * (2 * l1RB) * sizeof(C) <= 96 * 1024) l1RB *= 2;
+            if (!upload_table(l1P, &twP, err) || !upload_table(l1Q, &twQ, err)) return false;
+            plan1 = planP;   // unused by the long path; keeps the handle's plans defined
+        } else {
+            if (!make_plans(err)) return false;
+            if (!choose_row(nrows, &row_cfg, err)) return false;
+        }
         choose_two_level();
         if (g.dim >= 2 && !choose_strided(plan2, g.n2, g.m1 + 1, g.dim == 3 ? g.n3 : 1, &s2_cfg, err)) return false;
         if (g.dim >= 3 && !choose_strided(plan3, g.n3, g.m1 + 1, g.n2, &s3_cfg, err)) return false;

@@ -29,7 +29,7 @@ def _solve(torch, prob, precision, **kw):
 
 # solver order (second dimension 64/128/160/256/320) and reference order
 # (Stockham FP32 passes), 1D row passes
-@pytest.mark.parametrize("kind,dims", [("1d", (4096,)), ("2d", (64, 64)), ("2d", (96, 128)), ("3d", (32, 32, 32)),
+@pytest.mark.parametrize("kind,dims", [("1d", (4096,)), ("1d", (24000,)), ("2d", (64, 64)), ("2d", (96, 128)), ("3d", (32, 32, 32)),
                                        ("3d", (32, 64, 24)), ("3d", (64, 64, 64))])
 @pytest.mark.parametrize("cg_rtol", [1e-8, 1e-5])
 def test_mixed_matches_fp64(cuda, kind, dims, cg_rtol):

@@ -10,8 +10,9 @@ from conftest import REF_GRID
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
+# 1D rows above 4096 samples take the multi-CTA four-step path (M = P*Q)
 EXTRA = [(16384,), (1000,), (2 * 3 * 5 * 7 * 2,), (256, 256), (62, 82), (30, 42), (64, 64, 64), (32, 48, 40),
-         (14, 22, 26), (20, 30, 18)]
+         (14, 22, 26), (20, 30, 18), (8192,), (4374,), (2 * 2 * 3 * 5 * 7 * 11,), (24000,), (65536,), (2 ** 20,)]
 
 
 def relerr(a, b):
