@@ -498,6 +498,12 @@ def run_serving(args, n_req, slots, rank):
                 "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
                 "failed": int(sum(x.status != 0 for x in res))}
 
+    # untimed: the first slots' worth of requests through the server (device
+    # memory pool and per-size kernel set-up warm, as in a running service)
+    with Server(slots=slots) as srv:
+        for k, r in enumerate(reqs[:slots]):
+            srv.submit(r["size"], r["z0"], r["lam"], r["missing"], tag=k, precision=r["precision"], **opts)
+        srv.drain()
     closed = serve(0.0)
     poisson = serve(5.0 * seq_rate)
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("1d", "2d", "3d")}

@@ -349,6 +349,21 @@ class SolveResult:
         return self.solution[:n]
 
 
+def CompressedSensingADMM(parameters: FFTParameters, fft_operator: "FFTOperator", rho=1.0, maxt=1000, tol=1e-6):
+    """CompressedSensingADMM(fft_parameter, fft_operator; rho, maxt, tol) —
+    src/admm.jl:8-61, on the device (csipm_admm).  Returns z (torch, N); the
+    statistics land in ``fft_operator.admm_stats``."""
+    torch = _torch()
+    n = int(np.prod(parameters.DFTsize))
+    z = torch.empty(n, dtype=torch.float64, device=fft_operator.z0.device)
+    st = _native.AdmmStats()
+    status = lib().csipm_admm(fft_operator.handle, float(rho), int(maxt), float(tol), _ptr(z), ctypes.byref(st))
+    if status not in (0, _native.CSIPM_ERR_IPM_MAXITER):
+        check(status, fft_operator.handle)
+    fft_operator.admm_stats = st.as_dict()
+    return z
+
+
 def ipm_solve(nlp: FFTNLPModel, raise_on_error=False):
     """ipm_solve!(solver) — src/CompressedSensingIPM.jl:31-36, on the device."""
     torch = _torch()

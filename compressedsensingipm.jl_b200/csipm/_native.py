@@ -34,7 +34,7 @@ EXPORTS = (
     "csipm_apply_AtA", "csipm_obj", "csipm_grad", "csipm_cons", "csipm_hprod", "csipm_kkt_build",
     "csipm_condensed_mul", "csipm_precond_mul", "csipm_kkt_mul", "csipm_jtprod", "csipm_kkt_solve",
     "csipm_solve", "csipm_get_timers", "csipm_profile_passes", "csipm_apply_AtA_static", "csipm_trim_pool",
-    "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
+    "csipm_admm", "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
 )
 
 
@@ -84,6 +84,14 @@ class Stats(ctypes.Structure):
         ("launches", ctypes.c_longlong),
         ("fallbacks", ctypes.c_int),
     ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class AdmmStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("cg_iter", ctypes.c_int),
+                ("err", ctypes.c_double), ("solve_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -146,6 +154,7 @@ def load(path: str | None = None):
         "csipm_profile_passes": (I, [H, D, I, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.c_char_p, ctypes.POINTER(I)]),
         "csipm_apply_AtA_static": (I, [I, ctypes.POINTER(I), D, D, D, ctypes.c_void_p]),
         "csipm_trim_pool": (I, [I]),
+        "csipm_admm": (I, [H, dbl, I, dbl, D, ctypes.POINTER(AdmmStats)]),
         "csipm_footprint": (I, [I, ctypes.POINTER(I), I, ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)]),
         "csipm_server_create": (I, [ctypes.POINTER(ServerOptions), ctypes.POINTER(H)]),
         "csipm_server_submit": (I, [H, ctypes.POINTER(Request)]),

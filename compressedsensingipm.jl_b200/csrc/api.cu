@@ -2,6 +2,8 @@
 // points, the fused Schur-complement PCG and the device-resident
 // interior-point loop.  The NLPModels / KKT-plugin entry points are in
 // plugin.cu, the bit-exact maps in maps.cu.
+#include <limits>
+
 #include "internal.h"
 
 namespace {
@@ -740,6 +742,91 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     S.launches = h->launches - la0;
     if (stats) *stats = S;
     if (status == CSIPM_ERR_IPM_MAXITER) fail(h, status, "IPM reached max_iter before the tolerance");
+    return status;
+}
+
+int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, csipm_admm_stats* stats) {
+    if (!h || !z_out) return fail(h, CSIPM_ERR_INVALID, "null argument");
+    if (!(rho > 0.0) || maxt < 0) return fail(h, CSIPM_ERR_INVALID, "rho must be > 0 and maxt >= 0");
+    const long long n = h->N;
+    const int nb = ew_blocks(n);
+    cudaStream_t st = h->stream;
+    const double lam = h->lambda;
+    const double* bv = h->sorder ? h->bs : h->b;
+    const int ppp = passes_per_product(h->g);
+    const double krylov_tol = std::sqrt(std::numeric_limits<double>::epsilon());
+    csipm_admm_stats S{};
+    cudaEventRecord(h->ev0, st);
+    // x0 = z = ones and y = 0 in the reference packing (src/admm.jl:19-24),
+    // mapped to the solve's order
+    double* X[2] = {h->dba, h->db};
+    double* z = h->s1;
+    double* y = h->s2;
+    fill_kernel<<<nb, EW_THREADS, 0, st>>>(n, 1.0, h->sorder ? h->Qb : X[1]);
+    if (h->sorder) CK(to_solver_order(h->g, h->Qb, X[1], st));
+    CK(cudaMemcpyAsync(z, X[1], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(y, 0, sizeof(double) * n, st));
+    fill_kernel<<<nb, EW_THREADS, 0, st>>>(n, rho, h->Db);   // A'A + rho I through the CG epilogue's diagonal
+    admm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, z, y, rho, h->rhs);
+    CK(cudaGetLastError());
+    h->launches += 4;
+    double err = 1.0;
+    int t = 0;
+    int status = CSIPM_OK;
+    while (t < maxt && err > tol) {
+        double* x1 = X[t & 1];
+        const double* x0 = X[(t + 1) & 1];
+        // x-update: Krylov cg from zero, no preconditioner, atol = rtol = sqrt(eps) (src/admm.jl:35-37)
+        CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
+        CK(cudaMemsetAsync(x1, 0, sizeof(double) * n, st));
+        cg_init_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, h->rhs, (const double*)nullptr, 0, (const double*)nullptr,
+                                                        h->cg_r, h->cg_p, h->ws(h->slots + SL_DUMMY), h->cgs,
+                                                        krylov_tol, krylov_tol);
+        CK(cudaGetLastError());
+        h->launches += 1;
+        auto iteration = [&](cudaStream_t s, int it) -> cudaError_t {
+            EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
+            cudaError_t e = solve_AtA(h, h->cg_p, ep, &h->cgs->done, s);
+            if (e != cudaSuccess) return e;
+            cg_update_kernel<double, double><<<nb, EW_THREADS, 0, s>>>(n, it, x1, h->cg_r, h->cg_p, h->cg_q,
+                                                                       (const double*)nullptr,
+                                                                       h->ws(h->slots + SL_DUMMY), h->cgs);
+            cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, s>>>(n, it, h->cg_r, (const double*)nullptr, h->cg_p,
+                                                               h->cgs);
+            return cudaGetLastError();
+        };
+        {
+            const int r = cg_iterations(h, &h->admm_exec[t & 1], h->opt.cg_maxit, iteration, ppp + 2);
+            if (r) return r;
+        }
+        CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        S.cg_iter += h->hcgs->iters;
+        h->matvecs += h->hcgs->iters;
+        if (h->hcgs->breakdown) { status = fail(h, CSIPM_ERR_NONFINITE, "ADMM x-update CG breakdown"); break; }
+        // z-, y-updates, the three differences and the next right-hand side
+        admm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, x1, x0, z, y, rho, lam, h->rhs, h->ws(h->slots + SL_RED));
+        CK(cudaGetLastError());
+        h->launches += 1;
+        const int r = read_slots(h, SL_RED, 3);
+        if (r) return r;
+        err = std::max(std::sqrt(h->hslots[SL_RED]), std::max(std::sqrt(h->hslots[SL_RED + 1]),
+                                                               std::sqrt(h->hslots[SL_RED + 2])));
+        if (!std::isfinite(err)) { status = fail(h, CSIPM_ERR_NONFINITE, "non-finite ADMM iterate"); break; }
+        ++t;
+    }
+    if (h->sorder) CK(to_reference_order(h->g, z, z_out, st));
+    else CK(cudaMemcpyAsync(z_out, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    cudaEventRecord(h->ev1, st);
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    if (status == CSIPM_OK && err > tol) status = CSIPM_ERR_IPM_MAXITER;
+    S.status = status;
+    S.iterations = t;
+    S.err = err;
+    S.solve_ms = ms;
+    if (stats) *stats = S;
     return status;
 }
 

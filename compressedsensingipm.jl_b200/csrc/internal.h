@@ -116,6 +116,7 @@ struct csipm_handle_s {
     // vector, dba and db; FP32: one), captured on first use
     cudaGraphExec_t cg_exec64[2] = {nullptr, nullptr};
     cudaGraphExec_t cg_exec32 = nullptr;
+    cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
     bool graphs_off = false;        // a capture failed: plain launches
     int fallbacks = 0;              // mixed Newton solves finished in FP64 after an FP32 breakdown
 
@@ -133,6 +134,8 @@ struct csipm_handle_s {
         for (auto& g : cg_exec64)
             if (g) cudaGraphExecDestroy(g);
         if (cg_exec32) cudaGraphExecDestroy(cg_exec32);
+        for (auto& g : admm_exec)
+            if (g) cudaGraphExecDestroy(g);
         for (void* p : allocs) cudaFreeAsync(p, stream);
         allocs.clear();
         op64.release();

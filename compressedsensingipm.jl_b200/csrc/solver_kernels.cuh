@@ -348,6 +348,38 @@ static __global__ void ipm_update_kernel(long long n, double lam, double* __rest
     }
 }
 
+// ------------------------------------------------------------------ ADMM (src/admm.jl)
+// b = A'z0 + rho z - y
+static __global__ void admm_rhs_kernel(long long n, const double* __restrict__ bv, const double* __restrict__ z,
+                                       const double* __restrict__ y, double rho, double* __restrict__ b) {
+    CSIPM_GRID_LOOP(i, n) b[i] = bv[i] + rho * z[i] - y[i];
+}
+
+// z1 = soft(x1 + y0/rho, lambda/rho), y1 = y0 + rho (x1 - z1), the squared
+// norms of x1 - x0, y1 - y0, z1 - z0, and the next right-hand side
+// A'z0 + rho z1 - y1 (z, y updated in place)
+static __global__ void admm_update_kernel(long long n, const double* __restrict__ bv, const double* __restrict__ x1,
+                                          const double* __restrict__ x0, double* __restrict__ z,
+                                          double* __restrict__ y, double rho, double lam, double* __restrict__ b,
+                                          RedWorkspace ws) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const double thre = lam / rho;
+    CSIPM_GRID_LOOP(i, n) {
+        const double xv = x1[i], y0 = y[i], z0 = z[i];
+        const double v = xv + y0 / rho;
+        const double z1 = v > thre ? v - thre : (v < -thre ? v + thre : 0.0);
+        const double y1 = y0 + rho * (xv - z1);
+        const double dx = xv - x0[i], dy = y1 - y0, dz = z1 - z0;
+        acc[0] += dx * dx;
+        acc[1] += dy * dy;
+        acc[2] += dz * dz;
+        z[i] = z1;
+        y[i] = y1;
+        b[i] = bv[i] + rho * z1 - y1;
+    }
+    grid_reduce<3>(acc, ws, 0u, 0u);
+}
+
 // c = (s1 + s2)/2
 static __global__ void half_sum_kernel(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
                                        double* __restrict__ c) {

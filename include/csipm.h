@@ -259,6 +259,24 @@ CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elem
 CSIPM_API int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, const double* x, double* y,
                                      void* stream);
 
+/* ---------------------------------------------------------------- ADMM */
+typedef struct {
+    int status;                /* CSIPM_OK, or CSIPM_ERR_IPM_MAXITER when maxt ran out before tol */
+    int iterations;            /* ADMM iterations t */
+    int cg_iter;               /* CG iterations of all x-updates */
+    double err;                /* final max(|x1-x0|, |y1-y0|, |z1-z0|) */
+    double solve_ms;
+} csipm_admm_stats;
+
+/* CompressedSensingADMM(fft_parameter, fft_operator; rho, maxt, tol) —
+ * src/admm.jl:8-61 on the device: x0 = z = 1, y = 0; each iteration solves
+ * (A'A + rho I) x = A'z0 + rho z - y by CG from zero (no preconditioner,
+ * atol = rtol = sqrt(eps), cap cg_maxit), z = soft(x + y/rho, lambda/rho),
+ * y += rho (x - z), until max of the three 2-norm differences <= tol.
+ * z_out: N (device), the final z.  Uses the handle's IPM workspace (a later
+ * csipm_solve starts afresh). */
+CSIPM_API int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, csipm_admm_stats* stats);
+
 /* ---------------------------------------------------------------- serving */
 /* A request loop for many recoveries of uneven sizes (no counterpart in the
  * reference, which solves one recovery per call, src/CompressedSensingIPM.jl:31-36).
