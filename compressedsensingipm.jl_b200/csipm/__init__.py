@@ -337,6 +337,84 @@ class FFTKKTSystem:
         return w
 
 
+class GondzioNLPModel:
+    """GondzioNLPModel{VT}(parameters; krylov_solver, rdft, preconditioner) —
+    src/gondzio_model.jl:12-65: x = [p; q; r] (3N), beta = p - q, one
+    constraint block z0 - A(p - q) - r = 0.  obj/grad!/cons! on the device."""
+
+    def __init__(self, parameters: FFTParameters, krylov_solver="cg", rdft=False, preconditioner=True, **opts):
+        if krylov_solver != "cg":
+            raise ValueError("only krylov_solver='cg' is available")
+        self.parameters = parameters
+        self.op_fft = FFTOperator(parameters, rdft=rdft, preconditioner=preconditioner, **opts)
+        self.nbeta = self.op_fft.N
+        self.nvar = 3 * self.nbeta
+        self.ncon = self.nbeta
+        self.counters = {"neval_obj": 0, "neval_grad": 0, "neval_cons": 0}
+
+    @property
+    def handle(self):
+        return self.op_fft.handle
+
+    def obj(self, x):
+        self.counters["neval_obj"] += 1
+        f = ctypes.c_double()
+        check(lib().csipm_gondzio_obj(self.handle, _ptr(_as_dev64(x, "x")), ctypes.byref(f)), self.handle)
+        return f.value
+
+    def grad(self, x, g):
+        self.counters["neval_grad"] += 1
+        check(lib().csipm_gondzio_grad(self.handle, _ptr(_as_dev64(x, "x")), _ptr(g)), self.handle)
+        return g
+
+    def cons(self, x, c):
+        self.counters["neval_cons"] += 1
+        check(lib().csipm_gondzio_cons(self.handle, _ptr(_as_dev64(x, "x")), _ptr(c)), self.handle)
+        return c
+
+
+class GondzioKKTSystem:
+    """The MadNLP KKT plugin of src/gondzio_kkt.jl over a GondzioNLPModel:
+    build_kkt!, condensed and preconditioner mul!, the 4N KKT mul! body,
+    jtprod! and solve_kkt! (after MadNLP.reduce_rhs!)."""
+
+    def __init__(self, nlp: GondzioNLPModel):
+        self.nlp = nlp
+        self.krylov_iterations = []
+
+    @property
+    def handle(self):
+        return self.nlp.handle
+
+    def build_kkt(self, pr_diag):
+        check(lib().csipm_gondzio_kkt_build(self.handle, _ptr(_as_dev64(pr_diag, "pr_diag"))), self.handle)
+
+    def condensed_mul(self, y, x, alpha=1.0, beta=0.0):
+        check(lib().csipm_gondzio_condensed_mul(self.handle, _ptr(y), _ptr(_as_dev64(x, "x")), float(alpha),
+                                                float(beta)), self.handle)
+        return y
+
+    def precond_mul(self, y, x, alpha=1.0, beta=0.0):
+        check(lib().csipm_gondzio_precond_mul(self.handle, _ptr(y), _ptr(_as_dev64(x, "x")), float(alpha),
+                                              float(beta)), self.handle)
+        return y
+
+    def mul(self, y, x, alpha=1.0, beta=0.0):
+        check(lib().csipm_gondzio_kkt_mul(self.handle, _ptr(y), _ptr(_as_dev64(x, "x")), float(alpha), float(beta)),
+              self.handle)
+        return y
+
+    def jtprod(self, y, x):
+        check(lib().csipm_gondzio_jtprod(self.handle, _ptr(y), _ptr(_as_dev64(x, "x"))), self.handle)
+        return y
+
+    def solve_kkt(self, w):
+        it = ctypes.c_int()
+        check(lib().csipm_gondzio_kkt_solve(self.handle, _ptr(w), ctypes.byref(it)), self.handle)
+        self.krylov_iterations.append(int(it.value))
+        return w
+
+
 @dataclasses.dataclass
 class SolveResult:
     solution: object        # 2N tensor [beta; c]

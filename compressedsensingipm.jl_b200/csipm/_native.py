@@ -34,7 +34,9 @@ EXPORTS = (
     "csipm_apply_AtA", "csipm_obj", "csipm_grad", "csipm_cons", "csipm_hprod", "csipm_kkt_build",
     "csipm_condensed_mul", "csipm_precond_mul", "csipm_kkt_mul", "csipm_jtprod", "csipm_kkt_solve",
     "csipm_solve", "csipm_get_timers", "csipm_profile_passes", "csipm_apply_AtA_static", "csipm_trim_pool",
-    "csipm_admm", "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
+    "csipm_admm", "csipm_gondzio_obj", "csipm_gondzio_grad", "csipm_gondzio_cons", "csipm_gondzio_kkt_build",
+    "csipm_gondzio_condensed_mul", "csipm_gondzio_precond_mul", "csipm_gondzio_kkt_mul", "csipm_gondzio_jtprod",
+    "csipm_gondzio_kkt_solve", "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
 )
 
 
@@ -154,6 +156,15 @@ def load(path: str | None = None):
         "csipm_profile_passes": (I, [H, D, I, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.c_char_p, ctypes.POINTER(I)]),
         "csipm_apply_AtA_static": (I, [I, ctypes.POINTER(I), D, D, D, ctypes.c_void_p]),
         "csipm_trim_pool": (I, [I]),
+        "csipm_gondzio_obj": (I, [H, D, ctypes.POINTER(dbl)]),
+        "csipm_gondzio_grad": (I, [H, D, D]),
+        "csipm_gondzio_cons": (I, [H, D, D]),
+        "csipm_gondzio_kkt_build": (I, [H, D]),
+        "csipm_gondzio_condensed_mul": (I, [H, D, D, dbl, dbl]),
+        "csipm_gondzio_precond_mul": (I, [H, D, D, dbl, dbl]),
+        "csipm_gondzio_kkt_mul": (I, [H, D, D, dbl, dbl]),
+        "csipm_gondzio_jtprod": (I, [H, D, D]),
+        "csipm_gondzio_kkt_solve": (I, [H, D, ctypes.POINTER(I)]),
         "csipm_admm": (I, [H, dbl, I, dbl, D, ctypes.POINTER(AdmmStats)]),
         "csipm_footprint": (I, [I, ctypes.POINTER(I), I, ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)]),
         "csipm_server_create": (I, [ctypes.POINTER(ServerOptions), ctypes.POINTER(H)]),

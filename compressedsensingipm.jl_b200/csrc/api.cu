@@ -447,6 +447,7 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     h->g = make_geom(prob->dim, n, n[0] / 2 + 1);
     h->N = h->g.N;
     h->lambda = prob->lambda;
+    h->z0 = prob->z0;
     if (h->opt.cg_maxit <= 0) h->opt.cg_maxit = (int)std::min<long long>(2 * h->N, 1 << 30);
     auto bail = [&](int st, const std::string& m) { g_last_error = m; delete h; return st; };
     // NULL selects the CUDA default stream (the cuBLAS/cuFFT convention)

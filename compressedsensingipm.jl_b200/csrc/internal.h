@@ -109,6 +109,10 @@ struct csipm_handle_s {
     // KKT plugin (allocated on first use)
     double *L1 = nullptr, *L2 = nullptr, *P11 = nullptr, *P12 = nullptr, *P22 = nullptr;
     double *k_b = nullptr, *k_x = nullptr, *k_r = nullptr, *k_p = nullptr, *k_q = nullptr;
+    // Gondzio plugin (allocated on first use)
+    double *gz_Dp = nullptr, *gz_Dq = nullptr, *gz_P11 = nullptr, *gz_P12 = nullptr, *gz_P22 = nullptr;
+    double *gz_t1 = nullptr, *gz_t2 = nullptr;
+    const double* z0 = nullptr;     // the caller's z0 (FFTParameters.z0: outlives the handle)
     // mixed precision: FP32 copies of the Schur diagonal / preconditioner and the FP32 CG vectors
     float *f_Db = nullptr, *f_Minv = nullptr, *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_x = nullptr;
     int refinements = 0;
@@ -359,5 +363,6 @@ cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cu
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
 int ensure_kkt_buffers(csipm_handle h);
+int ensure_gondzio_buffers(csipm_handle h);
 
 }  // namespace csipm_internal

@@ -259,6 +259,32 @@ CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elem
 CSIPM_API int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, const double* x, double* y,
                                      void* stream);
 
+/* ---------------------------------------------------------------- Gondzio formulation */
+/* GondzioNLPModel / GondzioKKTSystem (src/gondzio_model.jl, src/gondzio_kkt.jl)
+ * on the same handle: beta = p - q, p, q >= 0, residual variable r,
+ * x = [p; q; r] (3N), constraint z0 - A(p - q) - r = 0 (N).  The handle keeps
+ * the problem's z0 pointer (FFTParameters.z0 outlives the model). */
+
+/* NLPModels.obj: 1/2 r'r + lambda sum(p, q) — src/gondzio_model.jl:67-78 */
+CSIPM_API int csipm_gondzio_obj(csipm_handle h, const double* x, double* f);
+/* NLPModels.grad!: g = [lambda (2N); r] — src/gondzio_model.jl:80-93 */
+CSIPM_API int csipm_gondzio_grad(csipm_handle h, const double* x, double* g);
+/* NLPModels.cons!: c = z0 - A(p - q) - r — src/gondzio_model.jl:95-110 */
+CSIPM_API int csipm_gondzio_cons(csipm_handle h, const double* x, double* c);
+/* build_kkt!: Dp, Dq from pr_diag[0:2N) and the block preconditioner — src/gondzio_kkt.jl:278-301 */
+CSIPM_API int csipm_gondzio_kkt_build(csipm_handle h, const double* pr_diag);
+/* CondensedGondzioKKTSystem mul!: y = alpha [A'A + Dp, -A'A; -A'A, A'A + Dq] x + beta y (2N) — src/gondzio_kkt.jl:28-53 */
+CSIPM_API int csipm_gondzio_condensed_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+/* GondzioPreconditioner mul! (2N) — src/gondzio_kkt.jl:82-93 */
+CSIPM_API int csipm_gondzio_precond_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+/* MadNLP.mul! body before _kktmul!, x, y = [p; q; r; y] (4N) — src/gondzio_kkt.jl:213-248 */
+CSIPM_API int csipm_gondzio_kkt_mul(csipm_handle h, double* y, const double* x, double alpha, double beta);
+/* jtprod!: y = [-A'x; A'x; -x] (3N), x: N — src/gondzio_kkt.jl:250-268 */
+CSIPM_API int csipm_gondzio_jtprod(csipm_handle h, double* y, const double* x);
+/* solve_kkt! after MadNLP.reduce_rhs!, w = [p; q; r; y] (4N) in place; PCG
+ * with the block preconditioner (cg_atol, cg_rtol) — src/gondzio_kkt.jl:303-362 */
+CSIPM_API int csipm_gondzio_kkt_solve(csipm_handle h, double* w, int* cg_iters);
+
 /* ---------------------------------------------------------------- ADMM */
 typedef struct {
     int status;                /* CSIPM_OK, or CSIPM_ERR_IPM_MAXITER when maxt ran out before tol */
