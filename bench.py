@@ -453,8 +453,9 @@ def run_serving(args, n_req, slots, rank):
     reqs = serving_problems(n_req, seed0=1000 + 100000 * rank)
     L = csipm.lib()
     # every request is solved to a relative duality gap of 1e-8; the serving
-    # loop uses inexact Newton solves (CG rtol 1e-3), robust on this mix
-    opts = dict(tol=1e-8, ipm_cg_rtol=SERVE_CG_RTOL)
+    # loop uses inexact Newton solves (CG rtol 1e-3), robust on this mix; the
+    # stream's sizes hardly repeat, so per-size autotuning could not amortise
+    opts = dict(tol=1e-8, ipm_cg_rtol=SERVE_CG_RTOL, autotune=False)
 
     def sequential(kw):
         torch.cuda.synchronize()
@@ -474,7 +475,7 @@ def run_serving(args, n_req, slots, rank):
         return n_req / (time.perf_counter() - t0), int(sum(s != 0 for s in status))
 
     seq_rate, seq_failed = sequential(opts)
-    seq_default_rate, seq_default_failed = sequential(dict(tol=1e-8))
+    seq_default_rate, seq_default_failed = sequential(dict(tol=1e-8, autotune=False))
 
     def serve(rate):
         rng = np.random.default_rng(7)

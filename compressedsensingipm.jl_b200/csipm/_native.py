@@ -67,6 +67,7 @@ class Options(ctypes.Structure):
         ("stream", ctypes.c_void_p),
         ("layout", ctypes.c_int),
         ("cuda_graphs", ctypes.c_int),
+        ("autotune", ctypes.c_int),
     ]
 
 

@@ -5,6 +5,7 @@
 #include <limits>
 
 #include "internal.h"
+#include "tune.cuh"
 
 namespace {
 thread_local std::string g_last_error;
@@ -417,6 +418,7 @@ int csipm_default_options(csipm_options* opt) {
     opt->ir_max = 3;
     opt->verbose = 0;
     opt->cuda_graphs = 1;
+    opt->autotune = 1;
     opt->stream = nullptr;
     return CSIPM_OK;
 }
@@ -484,6 +486,10 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     }
     if (dmiss) cudaFreeAsync(dmiss, h->stream);
     if (!ok) return bail(err.find("memory") != std::string::npos ? CSIPM_ERR_OOM : CSIPM_ERR_UNSUPPORTED, err);
+    if (h->opt.autotune) {
+        autotune(h->op64, h->stream);
+        if (mixed) autotune(h->op32, h->stream);
+    }
     // reduction workspace: enough partials for the largest grid
     size_t maxblocks = 8192;
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * (h->g.dim == 3 ? h->g.n3 : 1));

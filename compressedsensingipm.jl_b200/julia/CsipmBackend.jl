@@ -42,6 +42,7 @@ mutable struct CsipmOptions              # csipm_options
     stream::Ptr{Cvoid}
     layout::Cint
     cuda_graphs::Cint
+    autotune::Cint
 end
 
 mutable struct CsipmStats                # csipm_stats
@@ -68,7 +69,7 @@ function csipm_check(st, h=C_NULL)
 end
 
 function default_options(; rdft=true, mixed=false, tol=1e-8, ipm_cg_rtol=1e-8)
-    o = CsipmOptions(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, C_NULL, 0, 0)
+    o = CsipmOptions(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, C_NULL, 0, 0, 0)
     csipm_check(ccall((:csipm_default_options, libcsipm), Cint, (Ref{CsipmOptions},), o))
     o.rdft = rdft
     o.precision = mixed ? 1 : 0

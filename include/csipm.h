@@ -92,6 +92,10 @@ typedef struct {
     int cuda_graphs;           /* 1 (default): csipm_solve replays groups of CG iterations from CUDA
                                   graphs captured once per handle; 0: plain launches (same kernels,
                                   same results) */
+    int autotune;              /* 1 (default): csipm_create times the candidate launch configurations
+                                  of the FFT passes for this size (two-level vs Stockham kernels,
+                                  lines / rows per CTA) once per process and keeps the fastest;
+                                  0: the built-in heuristic */
 } csipm_options;
 
 /* Per-solve statistics (MadNLPExecutionStats analogue + the reference's timers,

@@ -106,3 +106,21 @@ def test_cuda_graph_replay_changes_nothing(cuda, kind, dims, precision):
     assert torch.equal(out[True].beta, out[False].beta)
     for key in ("ipm_iter", "cg_iter", "matvecs"):
         assert out[True].stats[key] == out[False].stats[key]
+
+
+@pytest.mark.parametrize("kind,dims", [("3d", (48, 40, 36)), ("2d", (100, 96)), ("3d", (32, 64, 24))])
+def test_autotuned_and_heuristic_configs_agree(cuda, kind, dims):
+    """The autotuner only picks among launch configurations of the same
+    transforms: both solves reach the same optimum."""
+    import csipm
+    torch = cuda
+    prob = _problem(kind, dims, seed=6)
+    size = prob.size
+    out = {}
+    for tune in (True, False):
+        params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+        nlp = csipm.FFTNLPModel(params, rdft=True, tol=1e-10, autotune=tune)
+        res = csipm.ipm_solve(nlp)
+        assert res.status == 0, res.stats
+        out[tune] = res.beta.cpu().numpy()
+    assert np.linalg.norm(out[True] - out[False]) <= 1e-7 * np.linalg.norm(out[False])
