@@ -108,48 +108,80 @@ cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cu
 // ------------------------------------------------------------------ CG iteration loop
 // Runs PCG iterations (iteration(stream, it) launches one; `it` only selects
 // the parity of the double-buffered scalars) until the device `done` flag is
-// read back set or maxit is reached.  From the third iteration on, groups of
-// CG_GRAPH_ITERS iterations are replayed from a CUDA graph captured once per
-// handle and vector (one launch instead of CG_GRAPH_ITERS x (passes + 2));
-// iterations after convergence return at once on the device flag.  The flag
-// is read back after 2, 4, then every 8 iterations.
-constexpr int CG_GRAPH_ITERS = 4;
+// set or maxit is reached.
+//
+// With CUDA graphs (the default) the whole loop is one graph launch: a
+// conditional WHILE node whose body is two iterations followed by a
+// one-thread kernel that keeps the loop going while `done` is clear and
+// fewer than CG_WHILE_CAP iterations ran (the bound keeps every device loop
+// finite); the graph is captured once per handle and solution vector.  The
+// host reads the scalars once at the end and finishes with plain launches
+// in the rare case the cap was reached.  Without graphs the flag is read
+// back after 2, 4, then every 8 iterations.
+constexpr int CG_WHILE_CAP = 2000;
+
+static __global__ void cg_continue_kernel(cudaGraphConditionalHandle hnd, const CgScalars* __restrict__ sc, int cap) {
+    cudaGraphSetConditional(hnd, (sc->done == 0 && sc->iters < cap) ? 1u : 0u);
+}
+
+template <class Iter>
+bool build_cg_while(csipm_handle h, cudaGraphExec_t* exec, int cap, Iter& iteration) {
+    cudaGraph_t graph = nullptr;
+    cudaStream_t cs = nullptr;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle hnd = 0;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&hnd, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node = nullptr;
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    if (ok) ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+             cudaSuccess;
+        if (ok) {
+            ok = iteration(cs, 0) == cudaSuccess && iteration(cs, 1) == cudaSuccess;
+            cg_continue_kernel<<<1, 1, 0, cs>>>(hnd, h->cgs, cap);
+            ok = cudaGetLastError() == cudaSuccess && ok;
+            cudaGraph_t out = nullptr;
+            ok = cudaStreamEndCapture(cs, &out) == cudaSuccess && ok;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(exec, graph, 0) == cudaSuccess;
+    if (cs) cudaStreamDestroy(cs);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (!ok) *exec = nullptr;
+    return ok;
+}
 
 template <class Iter>
 int cg_iterations(csipm_handle h, cudaGraphExec_t* exec, int maxit, Iter&& iteration, int per_iter) {
     cudaStream_t st = h->stream;
-    int it = 0, chunk = 2, since = 0;
-    while (it < maxit) {
-        int step = 1;
-        if (exec && h->opt.cuda_graphs && !h->graphs_off && it >= 2 && it % 2 == 0 && it + CG_GRAPH_ITERS <= maxit) {
-            if (!*exec) {
-                cudaStream_t cs = nullptr;
-                cudaGraph_t g = nullptr;
-                bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
-                          cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-                if (ok) {
-                    for (int k = 0; k < CG_GRAPH_ITERS && ok; ++k) ok = iteration(cs, k) == cudaSuccess;
-                    ok = (cudaStreamEndCapture(cs, &g) == cudaSuccess) && ok && g;
-                }
-                if (ok) ok = cudaGraphInstantiate(exec, g, 0) == cudaSuccess;
-                if (g) cudaGraphDestroy(g);
-                if (cs) cudaStreamDestroy(cs);
-                cudaGetLastError();
-                if (!ok) {
-                    *exec = nullptr;
-                    h->graphs_off = true;   // plain launches from now on
-                }
-            }
-            if (*exec) {
-                CK(cudaGraphLaunch(*exec, st));
-                step = CG_GRAPH_ITERS;
-            }
+    int it = 0;
+    if (exec && h->opt.cuda_graphs && !h->graphs_off && maxit >= 2) {
+        if (!*exec && !build_cg_while(h, exec, std::min(maxit, CG_WHILE_CAP), iteration)) h->graphs_off = true;
+        if (*exec) {
+            CK(cudaGraphLaunch(*exec, st));
+            CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            h->launches += (long long)h->hcgs->iters * per_iter + 1;
+            if (h->hcgs->done) return CSIPM_OK;
+            it = h->hcgs->iters;   // cap reached (even): continue with plain launches
         }
-        if (step == 1) CK(iteration(st, it));
-        h->launches += (long long)step * per_iter;
-        it += step;
-        since += step;
-        if (since >= chunk || it >= maxit) {
+    }
+    int chunk = 2, since = 0;
+    while (it < maxit) {
+        CK(iteration(st, it));
+        h->launches += per_iter;
+        ++it;
+        if (++since >= chunk || it >= maxit) {
             since = 0;
             if (chunk < 8) chunk *= 2;
             CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
@@ -692,36 +724,28 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
                        : schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, 0.0, h->dba,
+        // the centring target and the step length are computed on the device
+        // from the step statistics: no host round trip inside the iteration
+        double* sigmu_d = h->slots + SL_SIGMU;
+        double* alpha_d = h->slots + SL_ALPHA;
+        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, nullptr, h->dba,
                                                         h->ws(h->slots + SL_SS));
-        CK(cudaGetLastError());
-        r = read_slots(h, SL_SS, SS_N);
-        if (r) return r;
-        const double* Q = h->hslots + SL_SS;
-        double a = std::min(1.0, std::min(Q[SS_MINP], Q[SS_MIND]));
-        const double mu_aff = (Q[SS_SZ] + a * Q[SS_CROSS] + a * a * Q[SS_DD]) / (2.0 * (double)n);
-        const double sigma = std::pow(std::max(mu_aff, 0.0) / mu, 3.0);
-        const double sigmu = sigma * mu;
+        ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, mu, 2.0 * (double)n, sigmu_d);
         // ---- corrector
-        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba, sigmu, h->rhs);
+        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba, sigmu_d, h->rhs);
+        CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h->db, h->dba, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its)
                    : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu, h->db,
+        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,
                                                         h->ws(h->slots + SL_SS));
+        ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, std::max(0.99, 1.0 - mu), alpha_d);
+        ipm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d,
+                                                      h->db, alpha_d);
         CK(cudaGetLastError());
-        r = read_slots(h, SL_SS, SS_N);
-        if (r) return r;
-        const double eta = std::max(0.99, 1.0 - mu);
-        const double ap = std::min(1.0, eta * Q[SS_MINP]);
-        const double ad = std::min(1.0, eta * Q[SS_MIND]);
-        a = std::min(ap, ad);
-        ipm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu, h->db,
-                                                      a, a);
-        CK(cudaGetLastError());
-        h->launches += 4;   // corrector rhs, 2 step statistics, update (+ CG launches counted in the Newton solves)
+        h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, update (+ the Newton solves' launches)
     }
     if (c_out) {
         half_sum_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->s1, h->s2, h->c);

@@ -116,8 +116,8 @@ struct csipm_handle_s {
     // mixed precision: FP32 copies of the Schur diagonal / preconditioner and the FP32 CG vectors
     float *f_Db = nullptr, *f_Minv = nullptr, *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_x = nullptr;
     int refinements = 0;
-    // CUDA graphs of CG_GRAPH_ITERS CG iterations (FP64: one per solution
-    // vector, dba and db; FP32: one), captured on first use
+    // CUDA graphs of the whole CG loop (a conditional while node; FP64: one
+    // per solution vector, dba and db; FP32: one), captured on first use
     cudaGraphExec_t cg_exec64[2] = {nullptr, nullptr};
     cudaGraphExec_t cg_exec32 = nullptr;
     cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
@@ -184,7 +184,7 @@ inline int fail(csipm_handle h, int status, const std::string& msg) {
     } while (0)
 
 // slot indices in h->slots
-enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_COUNT = 64 };
+enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_SIGMU = 48, SL_ALPHA = 49, SL_COUNT = 64 };
 
 // ------------------------------------------------------------------ pass dispatch
 // Strided pass along `axis`: the two-level register kernel when the axis has

@@ -263,8 +263,9 @@ __device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, dou
 // second-order correction of the affine direction dba)
 static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2,
-                               const double* __restrict__ rd, const double* __restrict__ dba, double sigmu,
-                               double* __restrict__ rhs) {
+                               const double* __restrict__ rd, const double* __restrict__ dba,
+                               const double* __restrict__ sigmu_p, double* __restrict__ rhs) {
+    const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     CSIPM_GRID_LOOP(i, n) {
         const ElemPre e = elem_pre(s1v[i], s2v[i], z1[i], z2[i]);
         double cor1 = 0.0, cor2 = 0.0;
@@ -297,8 +298,9 @@ struct MinRatio {
 
 static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                      const double* __restrict__ z1, const double* __restrict__ z2,
-                                     const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
-                                     RedWorkspace ws) {
+                                     const double* __restrict__ dba, const double* __restrict__ sigmu_p,
+                                     const double* __restrict__ db, RedWorkspace ws) {
+    const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
     MinRatio mp, md;
     CSIPM_GRID_LOOP(i, n) {
@@ -324,11 +326,31 @@ static __global__ void ipm_stepstats_kernel(long long n, double lam, const doubl
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
 }
 
+// Centring target after the predictor (Mehrotra): a = min(1, primal and dual
+// ratios), mu_aff = (s'z + a cross + a^2 dd)/(2n), sigma = (mu_aff/mu)^3;
+// q: the predictor's step statistics.  One thread.
+static __global__ void ipm_sigma_kernel(const double* __restrict__ q, double mu, double two_n, double* __restrict__ sigmu) {
+    const double a = fmin(1.0, fmin(q[SS_MINP], q[SS_MIND]));
+    const double mu_aff = (q[SS_SZ] + a * q[SS_CROSS] + a * a * q[SS_DD]) / two_n;
+    const double r = fmax(mu_aff, 0.0) / mu;
+    *sigmu = r * r * r * mu;
+}
+
+// Step length after the corrector: min over primal and dual of
+// min(1, eta * ratio) (the same step for both).  One thread.
+static __global__ void ipm_alpha_kernel(const double* __restrict__ q, double eta, double* __restrict__ alpha) {
+    const double ap = fmin(1.0, eta * q[SS_MINP]);
+    const double ad = fmin(1.0, eta * q[SS_MIND]);
+    *alpha = fmin(ap, ad);
+}
+
 // beta += ap db ; s1 += ap ds1 ; s2 += ap ds2 ; z += ad dz
 static __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ s1v,
                                   double* __restrict__ s2v, double* __restrict__ z1, double* __restrict__ z2,
-                                  const double* __restrict__ dba, double sigmu, const double* __restrict__ db,
-                                  double ap, double ad) {
+                                  const double* __restrict__ dba, const double* __restrict__ sigmu_p,
+                                  const double* __restrict__ db, const double* __restrict__ alpha_p) {
+    const double sigmu = sigmu_p ? *sigmu_p : 0.0;
+    const double ap = *alpha_p, ad = ap;
     CSIPM_GRID_LOOP(i, n) {
         const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
         const ElemPre e = elem_pre(s1, s2, a, d);

@@ -89,9 +89,10 @@ typedef struct {
                                   "solver order" where the operator supports it (2D/3D), 1 the
                                   reference packing throughout.  Inputs and outputs of every entry
                                   point are in the reference packing either way. */
-    int cuda_graphs;           /* 1 (default): csipm_solve replays groups of CG iterations from CUDA
-                                  graphs captured once per handle; 0: plain launches (same kernels,
-                                  same results) */
+    int cuda_graphs;           /* 1 (default): every CG loop of csipm_solve / csipm_admm runs as one
+                                  CUDA graph launch (a conditional while node over the iterations,
+                                  captured once per handle); 0: plain launches (same kernels, same
+                                  results) */
     int autotune;              /* 1 (default): csipm_create times the candidate launch configurations
                                   of the FFT passes for this size (two-level vs Stockham kernels,
                                   lines / rows per CTA) once per process and keeps the fastest;
