@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="requests of the serving stream measured beside the headline solve (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="plain kernel launches instead of CUDA graphs (launch-list profiling sees every kernel)")
     ap.add_argument("--passes-only", action="store_true",
                     help="build the handle, launch each pass of one CG product twice (csipm_profile_passes, "
                          "reps=1), print the pass list and exit: the small command for kernel captures")
@@ -248,6 +250,8 @@ def run_ours(args):
     kw = dict(tol=args.tol)
     if args.cg_rtol is not None:
         kw["ipm_cg_rtol"] = args.cg_rtol
+    if args.no_graphs:
+        kw["cuda_graphs"] = False
     nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision, **kw)
     stream = torch.cuda.current_stream()
     if args.passes_only:

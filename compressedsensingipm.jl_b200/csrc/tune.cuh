@@ -29,6 +29,9 @@ struct TuneChoice {
 };
 
 constexpr int TUNE_REPS = 3;
+// a candidate replaces the incumbent only when it is this much faster
+// (timing noise must not flip between kernels of equal speed)
+constexpr float TUNE_MARGIN = 0.95f;
 
 using TuneKey = std::tuple<int, int, int, int, int, int>;   // sizeof(T), dim, n1, n2, n3, masked
 
@@ -159,7 +162,7 @@ void autotune(FftOperator<T>& op, cudaStream_t st) {
             const float t = tune_time<T>(st, e0, e1, [&] {
                 return run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 3, op.strided_args(3), (const double*)nullptr, none, st);
             });
-            if (t < t_best) { t_best = t; best.s3_two = 0; best.s3_tb = tb; }
+            if (t < TUNE_MARGIN * t_best) { t_best = t; best.s3_two = 0; best.s3_tb = tb; }
         }
         op.s3_A = A;
         op.s3_B = B;
@@ -179,7 +182,7 @@ void autotune(FftOperator<T>& op, cudaStream_t st) {
             const float t = tune_time<T>(st, e0, e1, [&] {
                 return run_strided<T, true, IN_SPEC, OUT_SPEC>(op, 2, op.strided_args(2), (const double*)nullptr, none, st);
             });
-            if (t < t_best) { t_best = t; best.s2_tb = tb; }
+            if (t < TUNE_MARGIN * t_best) { t_best = t; best.s2_tb = tb; }
         }
         op.s2_cfg = keep;
     }
@@ -204,7 +207,7 @@ void autotune(FftOperator<T>& op, cudaStream_t st) {
                 op.row_cfg = c;
                 ra = op.row_args(1.0, nullptr, nullptr);
                 const float t = tune_time<T>(st, e0, e1, row);
-                if (t < t_best) { t_best = t; best.row_two = 0; best.row_rb = rb; }
+                if (t < TUNE_MARGIN * t_best) { t_best = t; best.row_two = 0; best.row_rb = rb; }
             }
         }
         op.r_A = A;
