@@ -52,6 +52,29 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     const int ii = i0 + b;
     const bool interior = ii >= 1 && ii <= a.g.m1 - 1;
 
+    // Solver-order scatter: the epilogue operands of this thread's first
+    // SC_U outputs are requested now, so their latency hides behind step 1,
+    // the exchange and DFT_B (later chunks are prefetched one chunk ahead).
+    // FP32 only: in FP64 the extra live registers cost more occupancy than
+    // the early loads win.
+    constexpr int SC_U = 4;
+    constexpr bool SC_EARLY = sizeof(T) == 4;
+    typename Epi::Pre2 sc_pre[SC_U];
+    int64_t sc_p0 = 0, sc_ps = 0;
+    const bool sc_own = OUT == OUT_SSCATTER && t < A && live && interior;
+    if constexpr (OUT == OUT_SSCATTER) {
+        if (sc_own) {
+            int j0, k0s;
+            jk_of(a.jk_mode, o, t, j0, k0s);
+            sc_p0 = sol_pair(a.g, ii, j0, k0s);
+            sc_ps = (a.jk_mode == 0 ? (int64_t)a.g.n2 : (int64_t)1) * (a.g.m1 - 1) * A;
+            if constexpr (SC_EARLY) {
+#pragma unroll
+                for (int q = 0; q < SC_U; ++q)
+                    if (q < B) sc_pre[q] = epi.pre2(sc_p0 + q * sc_ps);
+            }
+        }
+    }
     // ---- step 1: thread t < B owns x = t + B*a
     if (t < B) {
         C v[A];
@@ -129,26 +152,39 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
 #pragma unroll
             for (int kb = 0; kb < B; ++kb) a.spec[base + (long long)(s + A * kb) * a.sx] = u[kb];
         } else if (OUT == OUT_SSCATTER && interior) {
-            constexpr int U = 4;
             // pair index of x = s + A*kb: one base plus kb times a fixed stride
-            int j0, k0s;
-            jk_of(a.jk_mode, o, s, j0, k0s);
-            const int64_t p0 = sol_pair(a.g, ii, j0, k0s);
-            const int64_t ps = (a.jk_mode == 0 ? (int64_t)a.g.n2 : (int64_t)1) * (a.g.m1 - 1) * A;
+            // (sc_p0, sc_ps); FP32 loads the operands one chunk ahead of their use
+            if constexpr (SC_EARLY) {
 #pragma unroll
-            for (int k0 = 0; k0 < B; k0 += U) {
-                int64_t l[U];
-                typename Epi::Pre2 pr[U];
+                for (int k0 = 0; k0 < B; k0 += SC_U) {
+                    typename Epi::Pre2 nxt[SC_U];
+                    if (k0 + SC_U < B) {
 #pragma unroll
-                for (int q = 0; q < U; ++q) {
-                    if (k0 + q < B) {
-                        l[q] = p0 + (k0 + q) * ps;
-                        pr[q] = ep.pre2(l[q]);
+                        for (int q = 0; q < SC_U; ++q)
+                            if (k0 + SC_U + q < B) nxt[q] = ep.pre2(sc_p0 + (k0 + SC_U + q) * sc_ps);
+                    }
+#pragma unroll
+                    for (int q = 0; q < SC_U; ++q)
+                        if (k0 + q < B)
+                            ep.put2(sc_p0 + (k0 + q) * sc_ps, (T)SQRT2_D * u[k0 + q].x, (T)SQRT2_D * u[k0 + q].y,
+                                    sc_pre[q]);
+                    if (k0 + SC_U < B) {
+#pragma unroll
+                        for (int q = 0; q < SC_U; ++q) sc_pre[q] = nxt[q];
                     }
                 }
+            } else {
 #pragma unroll
-                for (int q = 0; q < U; ++q)
-                    if (k0 + q < B) ep.put2(l[q], (T)SQRT2_D * u[k0 + q].x, (T)SQRT2_D * u[k0 + q].y, pr[q]);
+                for (int k0 = 0; k0 < B; k0 += SC_U) {
+#pragma unroll
+                    for (int q = 0; q < SC_U; ++q)
+                        if (k0 + q < B) sc_pre[q] = ep.pre2(sc_p0 + (k0 + q) * sc_ps);
+#pragma unroll
+                    for (int q = 0; q < SC_U; ++q)
+                        if (k0 + q < B)
+                            ep.put2(sc_p0 + (k0 + q) * sc_ps, (T)SQRT2_D * u[k0 + q].x, (T)SQRT2_D * u[k0 + q].y,
+                                    sc_pre[q]);
+                }
             }
         } else {
             constexpr int U = 2;
