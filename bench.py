@@ -102,7 +102,8 @@ class Dist:
             import datetime
             import torch.distributed as dist
             backend = "nccl" if use_gpu else "gloo"
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            # short: ranks that wait for a dead peer end with an error, not a hang
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.dist = dist
 
     def barrier(self):

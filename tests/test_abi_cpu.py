@@ -43,3 +43,29 @@ def test_invalid_sizes_rejected_without_gpu():
     st = L.csipm_beta_to_dft(2, n, 1, None, None, None)
     assert st == _native.CSIPM_ERR_ODD_DIM
     assert b"even" in L.csipm_last_error(None)
+
+
+def test_size_limits_and_footprint_without_gpu():
+    """N >= 2^31 is refused (32-bit indices on the device); csipm_footprint is
+    host arithmetic: it grows with the size and with mixed precision."""
+    from csipm import _native
+    L = _native.load()
+    big = (ctypes.c_int * 3)(2048, 2048, 1024)
+    out = ctypes.c_size_t()
+    assert L.csipm_footprint(3, big, 0, 0, ctypes.byref(out)) == _native.CSIPM_ERR_UNSUPPORTED
+    small = (ctypes.c_int * 3)(64, 64, 64)
+    mid = (ctypes.c_int * 3)(128, 128, 128)
+    f = []
+    for size, prec in ((small, 0), (mid, 0), (mid, 1)):
+        assert L.csipm_footprint(3, size, prec, 0, ctypes.byref(out)) == 0
+        f.append(out.value)
+    assert f[0] < f[1] < f[2]
+    assert f[1] >= 26 * 8 * 128 ** 3   # 24 FP64 vectors + the server's z0/beta staging
+
+
+def test_options_defaults_of_the_later_fields():
+    from csipm import _native
+    L = _native.load()
+    o = _native.Options()
+    assert L.csipm_default_options(ctypes.byref(o)) == 0
+    assert o.layout == 0 and o.cuda_graphs == 1 and o.autotune == 1 and o.precision == 0
