@@ -252,6 +252,16 @@ constexpr double MIXED_INNER_RTOL = 1e-6;
 constexpr double MIXED_FP32_WARM_RTOL = 1e-4;
 constexpr int MIXED_ROUND_MAXIT = 100;
 
+// FP64 Db/Minv of the current iterate, when the residual pass left them out
+static void ensure_diag64(csipm_handle h) {
+    if (!h->diag64_stale) return;
+    const long long n = h->N;
+    ipm_diag64_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, h->s1, h->s2, h->z1, h->z2, h->Db, h->Minv,
+                                                                   h->opt.preconditioner);
+    h->launches += 1;
+    h->diag64_stale = false;
+}
+
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
     const long long n = h->N;
     const int nb = ew_blocks(n);
@@ -270,6 +280,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         const double* res = rhs;
         double rin = std::max(rtol, MIXED_INNER_RTOL);
         if (round > 0 || (has_x0 && !fp32_warm)) {
+            ensure_diag64(h);
             EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
             CK(solve_AtA(h, x, ep, nullptr, st));
             resid64_kernel<<<nb, EW_THREADS, 0, st>>>(n, rhs, h->cg_q, Minv, h->cg_r, h->ws(h->slots + SL_DOT));
@@ -331,6 +342,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         CK(cudaGetLastError());
         h->launches += 1;
         if (h->hcgs->breakdown) {
+            ensure_diag64(h);
             int its = 0;
             const int r = schur_cg(h, rhs, x, true, std::min(0.5, rtol * r0 / rn), maxit, &its);
             total += its;
@@ -659,6 +671,9 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     const long long la0 = h->launches;
     const bool mixed = o.precision == CSIPM_MIXED;
     const int ppp = passes_per_product(h->g);
+    // mixed precision with a Newton tolerance the FP32 warm start serves:
+    // the FP64 barrier diagonals are only computed when a solve needs them
+    const bool lazy64 = mixed && o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL;
     cudaEventRecord(h->ev0, st);
     // every beta-space vector of the solve is in solver order when h->sorder
     const double* bv = h->sorder ? h->bs : h->b;
@@ -689,11 +704,14 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
             h->matvecs++;
             h->launches += ppp;
         }
-        h->launches += 1;   // residual + barrier diagonals + predictor right-hand side
-        ipm_resdiag_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
-                                                             h->rd, h->Db, h->Minv, mixed ? h->f_Db : nullptr,
-                                                             mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
-                                                             h->ws(h->slots + SL_RED));
+        h->launches += 1;   // pending s/z step + residual + barrier diagonals + predictor right-hand side
+        const bool step = k > 0;
+        h->diag64_stale = lazy64;
+        ipm_resdiag_kernel<float><<<nb, EW_THREADS, 0, st>>>(
+            n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2, step ? h->dba : nullptr, step ? h->db : nullptr,
+            h->slots + SL_SIGMU, h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
+            mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
+            h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
         int r = read_slots(h, SL_RED, RR_N);
         if (r) return r;
@@ -742,10 +760,11 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,
                                                         h->ws(h->slots + SL_SS));
         ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, std::max(0.99, 1.0 - mu), alpha_d);
-        ipm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->beta, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d,
-                                                      h->db, alpha_d);
+        // beta steps now (the next A'A product needs it); s and z take the
+        // same step inside the next residual pass
+        ipm_beta_step_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->beta, h->db, alpha_d);
         CK(cudaGetLastError());
-        h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, update (+ the Newton solves' launches)
+        h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, beta step (+ the Newton solves' launches)
     }
     if (c_out) {
         half_sum_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->s1, h->s2, h->c);

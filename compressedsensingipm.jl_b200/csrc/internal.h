@@ -122,6 +122,7 @@ struct csipm_handle_s {
     cudaGraphExec_t cg_exec32 = nullptr;
     cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
     bool graphs_off = false;        // a capture failed: plain launches
+    bool diag64_stale = false;      // FP64 Db/Minv not yet computed for this iterate (mixed precision)
     int fallbacks = 0;              // mixed Newton solves finished in FP64 after an FP32 breakdown
 
     // counters / timers

@@ -168,47 +168,6 @@ static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ 
     }
 }
 
-// One pass per interior-point iteration over the state: the dual residual
-// rd = Qb - b - z1 + z2 and the scalar diagnostics (reductions RR_*), the
-// barrier diagonals of the condensed Schur system Db = 4 D1 D2/(D1 + D2),
-// Minv = 1/(1 + Db) (FP32 copies for mixed precision), and the predictor
-// right-hand side (ipm_rhs_kernel with sigmu = 0 and no correction, where
-// h1 = -z1, h2 = -z2 and fc = -lambda).
-template <typename TV>
-static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb,
-                                          double lam, const double* __restrict__ beta, const double* __restrict__ s1v,
-                                          const double* __restrict__ s2v, const double* __restrict__ z1,
-                                          const double* __restrict__ z2, double* __restrict__ rd,
-                                          double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
-                                          TV* __restrict__ Minv_lo, int precond, double* __restrict__ rhs,
-                                          RedWorkspace ws) {
-    double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
-    CSIPM_GRID_LOOP(i, n) {
-        const double be = beta[i], s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i], q = Qb[i], bb = b[i];
-        const double ce = 0.5 * (s1 + s2);
-        const double r = q - bb - a + d;
-        rd[i] = r;
-        const double rc = lam - a - d;
-        acc[RR_SZ] += s1 * a + s2 * d;
-        acc[RR_BB] += bb * be;
-        acc[RR_BQB] += be * q;
-        acc[RR_L1] += fabs(be);
-        acc[RR_GINF] = fmax(acc[RR_GINF], fabs(bb - q));
-        acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
-        acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
-        acc[RR_SUMC] += ce;
-        const double D1 = a / s1, D2 = d / s2;
-        const double iL1 = 1.0 / (D1 + D2), L2 = D1 - D2;
-        const double dbv = 4.0 * D1 * D2 * iL1;
-        const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
-        Db[i] = dbv;
-        Minv[i] = mi;
-        if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
-        rhs[i] = -r - a + d + L2 * lam * iL1;
-    }
-    grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
-}
-
 // Per-element quantities shared by every direction of one iteration:
 // 1/s1, 1/s2, D1 = z1/s1, D2 = z2/s2, L2 = D1 - D2 and 1/L1 with L1 = D1 + D2
 // (three divisions; FP64 division is the expensive part of these kernels).
@@ -344,32 +303,6 @@ static __global__ void ipm_alpha_kernel(const double* __restrict__ q, double eta
     *alpha = fmin(ap, ad);
 }
 
-// beta += ap db ; s1 += ap ds1 ; s2 += ap ds2 ; z += ad dz
-static __global__ void ipm_update_kernel(long long n, double lam, double* __restrict__ beta, double* __restrict__ s1v,
-                                  double* __restrict__ s2v, double* __restrict__ z1, double* __restrict__ z2,
-                                  const double* __restrict__ dba, const double* __restrict__ sigmu_p,
-                                  const double* __restrict__ db, const double* __restrict__ alpha_p) {
-    const double sigmu = sigmu_p ? *sigmu_p : 0.0;
-    const double ap = *alpha_p, ad = ap;
-    CSIPM_GRID_LOOP(i, n) {
-        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
-        const ElemPre e = elem_pre(s1, s2, a, d);
-        const double dbi = db[i];
-        ElemDir o;
-        if (dba) {
-            const ElemDir f = elem_affine(e, lam, dba[i]);
-            o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, dbi);
-        } else {
-            o = elem_affine(e, lam, dbi);
-        }
-        beta[i] += ap * dbi;
-        s1v[i] = s1 + ap * o.ds1;
-        s2v[i] = s2 + ap * o.ds2;
-        z1[i] = a + ad * o.dz1;
-        z2[i] = d + ad * o.dz2;
-    }
-}
-
 // ------------------------------------------------------------------ ADMM (src/admm.jl)
 // b = A'z0 + rho z - y
 static __global__ void admm_rhs_kernel(long long n, const double* __restrict__ bv, const double* __restrict__ z,
@@ -400,6 +333,91 @@ static __global__ void admm_update_kernel(long long n, const double* __restrict_
         b[i] = bv[i] + rho * z1 - y1;
     }
     grid_reduce<3>(acc, ws, 0u, 0u);
+}
+
+// One pass per interior-point iteration over the state: first the pending
+// step of the previous iteration on the slacks and multipliers (beta was
+// stepped before the A'A product that produced Qb), when dba/db are given:
+// the corrector direction of each element recomputed from the stored
+// directions, s += alpha ds, z += alpha dz; then the dual residual
+// rd = Qb - b - z1 + z2 and the scalar diagnostics (reductions RR_*), the
+// barrier diagonals of the condensed Schur system Db = 4 D1 D2/(D1 + D2),
+// Minv = 1/(1 + Db) (FP64 when Db is given, FP32 copies for mixed
+// precision), and the predictor right-hand side (h1 = -z1, h2 = -z2,
+// fc = -lambda).
+template <typename TV>
+static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb,
+                                          double lam, const double* __restrict__ beta, double* __restrict__ s1v,
+                                          double* __restrict__ s2v, double* __restrict__ z1,
+                                          double* __restrict__ z2, const double* __restrict__ dba,
+                                          const double* __restrict__ db, const double* __restrict__ sigmu_p,
+                                          const double* __restrict__ alpha_p, double* __restrict__ rd,
+                                          double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
+                                          TV* __restrict__ Minv_lo, int precond, double* __restrict__ rhs,
+                                          RedWorkspace ws) {
+    double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const bool step = db != nullptr;
+    const double sigmu = step ? *sigmu_p : 0.0;
+    const double alpha = step ? *alpha_p : 0.0;
+    CSIPM_GRID_LOOP(i, n) {
+        double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
+        if (step) {
+            const ElemPre e = elem_pre(s1, s2, a, d);
+            const ElemDir f = elem_affine(e, lam, dba[i]);
+            const ElemDir o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, db[i]);
+            s1 += alpha * o.ds1;
+            s2 += alpha * o.ds2;
+            a += alpha * o.dz1;
+            d += alpha * o.dz2;
+            s1v[i] = s1;
+            s2v[i] = s2;
+            z1[i] = a;
+            z2[i] = d;
+        }
+        const double be = beta[i], q = Qb[i], bb = b[i];
+        const double ce = 0.5 * (s1 + s2);
+        const double r = q - bb - a + d;
+        rd[i] = r;
+        const double rc = lam - a - d;
+        acc[RR_SZ] += s1 * a + s2 * d;
+        acc[RR_BB] += bb * be;
+        acc[RR_BQB] += be * q;
+        acc[RR_L1] += fabs(be);
+        acc[RR_GINF] = fmax(acc[RR_GINF], fabs(bb - q));
+        acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
+        acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
+        acc[RR_SUMC] += ce;
+        const double D1 = a / s1, D2 = d / s2;
+        const double iL1 = 1.0 / (D1 + D2), L2 = D1 - D2;
+        const double dbv = 4.0 * D1 * D2 * iL1;
+        const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
+        if (Db) { Db[i] = dbv; Minv[i] = mi; }
+        if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
+        rhs[i] = -r - a + d + L2 * lam * iL1;
+    }
+    grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
+}
+
+// FP64 barrier diagonals alone (mixed precision at loose Newton tolerances
+// skips them in the residual pass; the first FP64 product or FP64 fallback
+// of the iteration computes them here)
+static __global__ void ipm_diag64_kernel(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
+                                         const double* __restrict__ z1, const double* __restrict__ z2,
+                                         double* __restrict__ Db, double* __restrict__ Minv, int precond) {
+    CSIPM_GRID_LOOP(i, n) {
+        const double D1 = z1[i] / s1[i], D2 = z2[i] / s2[i];
+        const double dbv = 4.0 * D1 * D2 * (1.0 / (D1 + D2));   // as in ipm_resdiag_kernel, bit for bit
+        Db[i] = dbv;
+        Minv[i] = precond ? 1.0 / (1.0 + dbv) : 1.0;
+    }
+}
+
+// beta += alpha db (the slacks and multipliers take their step in the next
+// residual pass)
+static __global__ void ipm_beta_step_kernel(long long n, double* __restrict__ beta, const double* __restrict__ db,
+                                            const double* __restrict__ alpha_p) {
+    const double alpha = *alpha_p;
+    CSIPM_GRID_LOOP(i, n) beta[i] += alpha * db[i];
 }
 
 // c = (s1 + s2)/2
