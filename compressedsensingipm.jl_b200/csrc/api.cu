@@ -194,19 +194,25 @@ int cg_iterations(csipm_handle h, cudaGraphExec_t* exec, int maxit, Iter&& itera
 
 // ------------------------------------------------------------------ Schur PCG
 // Solves (A'A + Db) x = rhs with preconditioner Minv (csipm_solve's inner solve).
-int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
+int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
+             const double* r0v) {
     const long long n = h->N;
     const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const double* Minv = h->opt.preconditioner ? h->Minv : nullptr;
+    h->resid_kind = RESID_NONE;
     CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
     const int ppp = passes_per_product(h->g);
-    if (has_x0) {
+    const bool given = has_x0 && r0v != nullptr;
+    if (given) {
+        rhs = r0v;       // r = rhs - K x0 given: CG on it from x0 with no product
+        has_x0 = false;
+    } else if (has_x0) {
         EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
         CK(solve_AtA(h, x, ep, nullptr, st));
         h->matvecs++;
         h->launches += ppp;
-    } else {
+    } else if (!given) {
         CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     }
     cg_init_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, rhs, h->cg_q, has_x0 ? 1 : 0, Minv, h->cg_r, h->cg_p,
@@ -231,6 +237,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
     h->matvecs += h->hcgs->iters;
     *iters = h->hcgs->iters;
     if (h->hcgs->breakdown) return fail(h, CSIPM_ERR_NONFINITE, "CG breakdown (non-positive curvature or non-finite value)");
+    h->resid_kind = RESID_CG64;   // x and r were updated together: r = rhs - K x up to rounding
     if (!h->hcgs->done) return CSIPM_ERR_CG_MAXITER;
     return CSIPM_OK;
 }
@@ -262,7 +269,8 @@ static void ensure_diag64(csipm_handle h) {
     h->diag64_stale = false;
 }
 
-int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters) {
+int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
+                const double* r0v) {
     const long long n = h->N;
     const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
@@ -274,12 +282,15 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
     double r0 = -1.0, rn = -1.0;
     // loose Newton tolerances take the warm-start residual from the FP32
     // product: its rounding (~1e-7 relative) is far below what they ask
-    const bool fp32_warm = has_x0 && rtol >= MIXED_FP32_WARM_RTOL;
+    // a given warm-start residual serves round 0 with no product at all
+    const bool given = has_x0 && r0v != nullptr;
+    const bool fp32_warm = has_x0 && !given && rtol >= MIXED_FP32_WARM_RTOL;
+    h->resid_kind = RESID_NONE;
     if (!has_x0) CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     for (int round = 0;; ++round) {
-        const double* res = rhs;
+        const double* res = given && round == 0 ? r0v : rhs;
         double rin = std::max(rtol, MIXED_INNER_RTOL);
-        if (round > 0 || (has_x0 && !fp32_warm)) {
+        if (round > 0 || (has_x0 && !fp32_warm && !given)) {
             ensure_diag64(h);
             EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
             CK(solve_AtA(h, x, ep, nullptr, st));
@@ -294,8 +305,10 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             if (round == 0) {
                 r0 = rn;
             } else {
-                if (rn <= rtol * r0) break;
-                if (round > h->opt.ir_max) break;
+                if (rn <= rtol * r0 || round > h->opt.ir_max) {
+                    h->resid_kind = RESID_CG64;
+                    break;
+                }
                 h->refinements++;
                 rin = std::min(0.5, std::max(MIXED_INNER_RTOL, rtol * r0 / rn));
             }
@@ -350,7 +363,10 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             *iters = total;
             return r;
         }
-        if (rtol >= MIXED_INNER_RTOL && round == 0 && h->hcgs->done) break;
+        if (rtol >= MIXED_INNER_RTOL && round == 0 && h->hcgs->done) {
+            h->resid_kind = RESID_F32;   // f_r = res - K32 d with x = x0 + d
+            break;
+        }
     }
     *iters = total;
     return CSIPM_OK;
@@ -749,12 +765,23 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, nullptr, h->dba,
                                                         h->ws(h->slots + SL_SS));
         ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, mu, 2.0 * (double)n, sigmu_d);
-        // ---- corrector
-        ipm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba, sigmu_d, h->rhs);
+        // ---- corrector, warm-started at dba.  Its starting residual
+        // rhs_c - K dba = rhs_c - rhs_p + (rhs_p - K dba) comes from the
+        // predictor solve's residual (kept by CG's recurrence) with no
+        // product; mixed precision at tight Newton tolerances computes it
+        // with an FP64 product instead, as refinement wants.
+        const int rk = (!mixed || o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL) ? h->resid_kind : RESID_NONE;
+        if (rk == RESID_F32)
+            ipm_rhs_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
+                                                             sigmu_d, h->rhs, h->f_r, h->db);
+        else
+            ipm_rhs_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
+                                                              sigmu_d, h->rhs, rk == RESID_CG64 ? h->cg_r : nullptr,
+                                                              h->db);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(h->db, h->dba, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its)
-                   : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its);
+        const double* r0v = rk != RESID_NONE ? h->rd : nullptr;
+        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v)
+                   : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
         ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,

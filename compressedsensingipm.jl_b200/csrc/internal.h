@@ -123,6 +123,7 @@ struct csipm_handle_s {
     cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
     bool graphs_off = false;        // a capture failed: plain launches
     bool diag64_stale = false;      // FP64 Db/Minv not yet computed for this iterate (mixed precision)
+    int resid_kind = 0;             // where the last Newton solve left rhs - K x (RESID_*)
     int fallbacks = 0;              // mixed Newton solves finished in FP64 after an FP32 breakdown
 
     // counters / timers
@@ -361,8 +362,16 @@ cudaError_t solve_AtA32(csipm_handle h, const float* x, const Epi& epi, const in
 cudaError_t to_solver_order(const Geom& g, const double* ref, double* sol, cudaStream_t st);
 cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cudaStream_t st);
 
-int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
-int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters);
+enum { RESID_NONE = 0, RESID_CG64 = 1, RESID_F32 = 2 };   // none / FP64 in cg_r / FP32 in f_r
+
+// Newton solves of the condensed system K x = rhs.  has_x0: x holds a start;
+// r0v (optional, with has_x0): rhs - K x0 is already known and no product
+// is spent on it.  On return h->resid_kind says where the residual
+// rhs - K x of the result is held (RESID_*).
+int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
+             const double* r0v = nullptr);
+int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
+                const double* r0v = nullptr);
 int ensure_kkt_buffers(csipm_handle h);
 int ensure_gondzio_buffers(csipm_handle h);
 

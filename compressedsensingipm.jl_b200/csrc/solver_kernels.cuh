@@ -219,11 +219,16 @@ __device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, dou
 }
 
 // rhs = fb - L2 fc / L1 with fb = -rd + h1 - h2 (corrector: sigmu and the
-// second-order correction of the affine direction dba)
+// second-order correction of the affine direction dba).  With rp (the
+// predictor solve's residual rhs_p - K dba) the corrector's warm-start
+// residual rhs - K dba = rhs - rhs_p + rp replaces rd (rd is not needed after
+// this pass; rhs still holds rhs_p on entry); with x0 the warm start
+// x0 = dba is written as well.
+template <typename TR>
 static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
-                               const double* __restrict__ z1, const double* __restrict__ z2,
-                               const double* __restrict__ rd, const double* __restrict__ dba,
-                               const double* __restrict__ sigmu_p, double* __restrict__ rhs) {
+                               const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
+                               const double* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
+                               const TR* __restrict__ rp, double* __restrict__ x0) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     CSIPM_GRID_LOOP(i, n) {
         const ElemPre e = elem_pre(s1v[i], s2v[i], z1[i], z2[i]);
@@ -237,7 +242,10 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
         const double h2 = (sigmu - cor2) * e.is2 - e.d;
         const double fb = -rd[i] + h1 - h2;
         const double fc = -(lam - e.a - e.d) + h1 + h2;
-        rhs[i] = fb - e.L2 * fc * e.iL1;
+        const double rn = fb - e.L2 * fc * e.iL1;
+        if (rp) rd[i] = rn - rhs[i] + (double)rp[i];
+        rhs[i] = rn;
+        if (x0) x0[i] = dba[i];
     }
 }
 
