@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
     ap.add_argument("--no-graphs", action="store_true",
                     help="plain kernel launches instead of CUDA graphs (launch-list profiling sees every kernel)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default pass variants instead of the per-size autotuner (profilers distort its timings)")
     ap.add_argument("--passes-only", action="store_true",
                     help="build the handle, launch each pass of one CG product twice (csipm_profile_passes, "
                          "reps=1), print the pass list and exit: the small command for kernel captures")
@@ -253,6 +255,8 @@ def run_ours(args):
         kw["ipm_cg_rtol"] = args.cg_rtol
     if args.no_graphs:
         kw["cuda_graphs"] = False
+    if args.no_autotune:
+        kw["autotune"] = False
     nlp = csipm.FFTNLPModel(params, rdft=True, precision=args.precision, **kw)
     stream = torch.cuda.current_stream()
     if args.passes_only:

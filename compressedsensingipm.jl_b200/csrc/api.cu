@@ -3,6 +3,7 @@
 // interior-point loop.  The NLPModels / KKT-plugin entry points are in
 // plugin.cu, the bit-exact maps in maps.cu.
 #include <limits>
+#include <mutex>
 
 #include "internal.h"
 #include "tune.cuh"
@@ -194,10 +195,33 @@ int cg_iterations(csipm_handle h, cudaGraphExec_t* exec, int maxit, Iter&& itera
 
 // ------------------------------------------------------------------ Schur PCG
 // Solves (A'A + Db) x = rhs with preconditioner Minv (csipm_solve's inner solve).
+int ew_grid(const void* kernel, long long n) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> cache;   // kernel -> CTAs per wave
+    int wave = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& e : cache)
+            if (e.first == kernel) { wave = e.second; break; }
+        if (!wave) {
+            int dev = 0, sms = 0, per_sm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, EW_THREADS, 0) != cudaSuccess) {
+                cudaGetLastError();
+                per_sm = 0;
+            }
+            wave = std::max(1, sms > 0 ? sms : 148) * std::max(1, per_sm);
+            cache.emplace_back(kernel, wave);
+        }
+    }
+    const long long b = (n + EW_THREADS - 1) / EW_THREADS;
+    return (int)std::max(1LL, std::min(b, (long long)wave));
+}
+
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
              const double* r0v) {
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const double* Minv = h->opt.preconditioner ? h->Minv : nullptr;
     h->resid_kind = RESID_NONE;
@@ -215,7 +239,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
     } else if (!given) {
         CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     }
-    cg_init_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, rhs, h->cg_q, has_x0 ? 1 : 0, Minv, h->cg_r, h->cg_p,
+    ew_launch(cg_init_kernel<double>, n, st, n, rhs, h->cg_q, has_x0 ? 1 : 0, Minv, h->cg_r, h->cg_p,
                                                     h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rtol);
     CK(cudaGetLastError());
     h->launches += 1;
@@ -223,9 +247,9 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
         EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
         cudaError_t e = solve_AtA(h, h->cg_p, ep, &h->cgs->done, s);
         if (e != cudaSuccess) return e;
-        cg_update_kernel<double, double><<<nb, EW_THREADS, 0, s>>>(n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
+        ew_launch(cg_update_kernel<double, double>, n, s, n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
                                                                    h->ws(h->slots + SL_DUMMY), h->cgs);
-        cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, s>>>(n, it, h->cg_r, Minv, h->cg_p, h->cgs);
+        ew_launch(cg_pupdate_kernel<double>, n, s, n, it, h->cg_r, Minv, h->cg_p, h->cgs);
         return cudaGetLastError();
     };
     // x is a kernel argument: a graph is only valid for the vector it was captured with
@@ -263,7 +287,7 @@ constexpr int MIXED_ROUND_MAXIT = 100;
 static void ensure_diag64(csipm_handle h) {
     if (!h->diag64_stale) return;
     const long long n = h->N;
-    ipm_diag64_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, h->s1, h->s2, h->z1, h->z2, h->Db, h->Minv,
+    ew_launch(ipm_diag64_kernel, n, h->stream, n, h->s1, h->s2, h->z1, h->z2, h->Db, h->Minv,
                                                                    h->opt.preconditioner);
     h->launches += 1;
     h->diag64_stale = false;
@@ -272,7 +296,6 @@ static void ensure_diag64(csipm_handle h) {
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
                 const double* r0v) {
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
     const double* Minv = pc ? h->Minv : nullptr;
@@ -294,7 +317,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             ensure_diag64(h);
             EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
             CK(solve_AtA(h, x, ep, nullptr, st));
-            resid64_kernel<<<nb, EW_THREADS, 0, st>>>(n, rhs, h->cg_q, Minv, h->cg_r, h->ws(h->slots + SL_DOT));
+            ew_launch(resid64_kernel, n, st, n, rhs, h->cg_q, Minv, h->cg_r, h->ws(h->slots + SL_DOT));
             CK(cudaGetLastError());
             h->matvecs++;
             h->launches += ppp + 1;
@@ -319,15 +342,15 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         CK(cudaMemsetAsync(h->f_x, 0, sizeof(float) * n, st));
         if (round == 0 && fp32_warm) {
             // warm-start residual rhs - K x0 with the FP32 product (x0 rounded to FP32)
-            convert_kernel<double, float><<<nb, EW_THREADS, 0, st>>>(n, x, h->f_p);
+            ew_launch(convert_kernel<double, float>, n, st, n, x, h->f_p);
             EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(h->slots + SL_DUMMY), 0.0};
             CK(solve_AtA32(h, h->f_p, ep, nullptr, st));
             h->matvecs++;
             h->launches += ppp + 1;
-            cg_init_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, rhs, h->f_q, 1, Minv32, h->f_r, h->f_p,
+            ew_launch(cg_init_kernel<float>, n, st, n, rhs, h->f_q, 1, Minv32, h->f_r, h->f_p,
                                                              h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
         } else {
-            cg_init_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, res, (const float*)nullptr, 0, Minv32, h->f_r, h->f_p,
+            ew_launch(cg_init_kernel<float>, n, st, n, res, (const float*)nullptr, 0, Minv32, h->f_r, h->f_p,
                                                              h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
         }
         CK(cudaGetLastError());
@@ -337,9 +360,9 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
             cudaError_t e = solve_AtA32(h, h->f_p, ep, &h->cgs->done, s);
             if (e != cudaSuccess) return e;
-            cg_update_kernel<float, float><<<nb, EW_THREADS, 0, s>>>(n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
+            ew_launch(cg_update_kernel<float, float>, n, s, n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
                                                                     h->ws(h->slots + SL_DUMMY), h->cgs);
-            cg_pupdate_kernel<float><<<nb, EW_THREADS, 0, s>>>(n, it, h->f_r, Minv32, h->f_p, h->cgs);
+            ew_launch(cg_pupdate_kernel<float>, n, s, n, it, h->f_r, Minv32, h->f_p, h->cgs);
             return cudaGetLastError();
         };
         {
@@ -351,7 +374,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         h->matvecs += h->hcgs->iters;
         total += h->hcgs->iters;
         if (r0 < 0.0) r0 = rn = std::sqrt(h->hcgs->rz0);   // |rhs| in the M-norm
-        add_f32_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->f_x, x);
+        ew_launch(add_f32_kernel, n, st, n, h->f_x, x);
         CK(cudaGetLastError());
         h->launches += 1;
         if (h->hcgs->breakdown) {
@@ -583,7 +606,7 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         cudaError_t e0 = op_At(h->op64, prob->z0, st_b, h->stream);
         if (e0 != cudaSuccess) return bail(CSIPM_ERR_CUDA, std::string("A^T z0 failed: ") + cudaGetErrorString(e0));
     }
-    dot2_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, prob->z0, prob->z0, nullptr, nullptr, h->ws(h->slots + SL_DOT));
+    ew_launch(dot2_kernel, h->N, h->stream, h->N, prob->z0, prob->z0, nullptr, nullptr, h->ws(h->slots + SL_DOT));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bail(CSIPM_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
     if (cudaMemcpyAsync(h->hslots + SL_DOT, h->slots + SL_DOT, sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
@@ -676,7 +699,6 @@ int csipm_apply_AtA(csipm_handle h, const double* x, double* y) {
 int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* stats) {
     if (!h || !beta_out) return fail(h, CSIPM_ERR_INVALID, "null argument");
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const double lam = h->lambda;
     const csipm_options& o = h->opt;
@@ -694,7 +716,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     // every beta-space vector of the solve is in solver order when h->sorder
     const double* bv = h->sorder ? h->bs : h->b;
     // ---- initial point: beta = soft(A^T z0, lambda), z from the clipped gradient, c balanced
-    ipm_init1_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, lam, h->beta, h->ws(h->slots + SL_MAXB));
+    ew_launch(ipm_init1_kernel, n, st, n, bv, lam, h->beta, h->ws(h->slots + SL_MAXB));
     CK(cudaGetLastError());
     {
         EpiStore<double> ep{h->Qb};
@@ -702,7 +724,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         h->matvecs++;
     }
     h->launches += 2 + ppp;
-    ipm_init2_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->s1, h->s2, h->z1,
+    ew_launch(ipm_init2_kernel, n, st, n, bv, h->Qb, lam, h->beta, h->slots + SL_MAXB, h->s1, h->s2, h->z1,
                                                  h->z2);
     CK(cudaGetLastError());
     {
@@ -723,7 +745,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         h->launches += 1;   // pending s/z step + residual + barrier diagonals + predictor right-hand side
         const bool step = k > 0;
         h->diag64_stale = lazy64;
-        ipm_resdiag_kernel<float><<<nb, EW_THREADS, 0, st>>>(
+        ew_launch(ipm_resdiag_kernel<float>, n, st, 
             n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2, step ? h->dba : nullptr, step ? h->db : nullptr,
             h->slots + SL_SIGMU, h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
             mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
@@ -762,7 +784,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         // from the step statistics: no host round trip inside the iteration
         double* sigmu_d = h->slots + SL_SIGMU;
         double* alpha_d = h->slots + SL_ALPHA;
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, nullptr, h->dba,
+        ew_launch(ipm_stepstats_kernel, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, nullptr, h->dba,
                                                         h->ws(h->slots + SL_SS));
         ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, mu, 2.0 * (double)n, sigmu_d);
         // ---- corrector, warm-started at dba.  Its starting residual
@@ -772,10 +794,10 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         // with an FP64 product instead, as refinement wants.
         const int rk = (!mixed || o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL) ? h->resid_kind : RESID_NONE;
         if (rk == RESID_F32)
-            ipm_rhs_kernel<float><<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
+            ew_launch(ipm_rhs_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
                                                              sigmu_d, h->rhs, h->f_r, h->db);
         else
-            ipm_rhs_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
+            ew_launch(ipm_rhs_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
                                                               sigmu_d, h->rhs, rk == RESID_CG64 ? h->cg_r : nullptr,
                                                               h->db);
         CK(cudaGetLastError());
@@ -784,17 +806,17 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
                    : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ipm_stepstats_kernel<<<nb, EW_THREADS, 0, st>>>(n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,
+        ew_launch(ipm_stepstats_kernel, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,
                                                         h->ws(h->slots + SL_SS));
         ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, std::max(0.99, 1.0 - mu), alpha_d);
         // beta steps now (the next A'A product needs it); s and z take the
         // same step inside the next residual pass
-        ipm_beta_step_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->beta, h->db, alpha_d);
+        ew_launch(ipm_beta_step_kernel, n, st, n, h->beta, h->db, alpha_d);
         CK(cudaGetLastError());
         h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, beta step (+ the Newton solves' launches)
     }
     if (c_out) {
-        half_sum_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->s1, h->s2, h->c);
+        ew_launch(half_sum_kernel, n, st, n, h->s1, h->s2, h->c);
         CK(cudaGetLastError());
         h->launches += 1;
     }
@@ -826,7 +848,6 @@ int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, 
     if (!h || !z_out) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!(rho > 0.0) || maxt < 0) return fail(h, CSIPM_ERR_INVALID, "rho must be > 0 and maxt >= 0");
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const double lam = h->lambda;
     const double* bv = h->sorder ? h->bs : h->b;
@@ -839,12 +860,12 @@ int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, 
     double* X[2] = {h->dba, h->db};
     double* z = h->s1;
     double* y = h->s2;
-    fill_kernel<<<nb, EW_THREADS, 0, st>>>(n, 1.0, h->sorder ? h->Qb : X[1]);
+    ew_launch(fill_kernel, n, st, n, 1.0, h->sorder ? h->Qb : X[1]);
     if (h->sorder) CK(to_solver_order(h->g, h->Qb, X[1], st));
     CK(cudaMemcpyAsync(z, X[1], sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(y, 0, sizeof(double) * n, st));
-    fill_kernel<<<nb, EW_THREADS, 0, st>>>(n, rho, h->Db);   // A'A + rho I through the CG epilogue's diagonal
-    admm_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, z, y, rho, h->rhs);
+    ew_launch(fill_kernel, n, st, n, rho, h->Db);   // A'A + rho I through the CG epilogue's diagonal
+    ew_launch(admm_rhs_kernel, n, st, n, bv, z, y, rho, h->rhs);
     CK(cudaGetLastError());
     h->launches += 4;
     double err = 1.0;
@@ -856,7 +877,7 @@ int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, 
         // x-update: Krylov cg from zero, no preconditioner, atol = rtol = sqrt(eps) (src/admm.jl:35-37)
         CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
         CK(cudaMemsetAsync(x1, 0, sizeof(double) * n, st));
-        cg_init_kernel<double><<<nb, EW_THREADS, 0, st>>>(n, h->rhs, (const double*)nullptr, 0, (const double*)nullptr,
+        ew_launch(cg_init_kernel<double>, n, st, n, h->rhs, (const double*)nullptr, 0, (const double*)nullptr,
                                                         h->cg_r, h->cg_p, h->ws(h->slots + SL_DUMMY), h->cgs,
                                                         krylov_tol, krylov_tol);
         CK(cudaGetLastError());
@@ -865,10 +886,10 @@ int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, 
             EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
             cudaError_t e = solve_AtA(h, h->cg_p, ep, &h->cgs->done, s);
             if (e != cudaSuccess) return e;
-            cg_update_kernel<double, double><<<nb, EW_THREADS, 0, s>>>(n, it, x1, h->cg_r, h->cg_p, h->cg_q,
+            ew_launch(cg_update_kernel<double, double>, n, s, n, it, x1, h->cg_r, h->cg_p, h->cg_q,
                                                                        (const double*)nullptr,
                                                                        h->ws(h->slots + SL_DUMMY), h->cgs);
-            cg_pupdate_kernel<double><<<nb, EW_THREADS, 0, s>>>(n, it, h->cg_r, (const double*)nullptr, h->cg_p,
+            ew_launch(cg_pupdate_kernel<double>, n, s, n, it, h->cg_r, (const double*)nullptr, h->cg_p,
                                                                h->cgs);
             return cudaGetLastError();
         };
@@ -882,7 +903,7 @@ int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, 
         h->matvecs += h->hcgs->iters;
         if (h->hcgs->breakdown) { status = fail(h, CSIPM_ERR_NONFINITE, "ADMM x-update CG breakdown"); break; }
         // z-, y-updates, the three differences and the next right-hand side
-        admm_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, bv, x1, x0, z, y, rho, lam, h->rhs, h->ws(h->slots + SL_RED));
+        ew_launch(admm_update_kernel, n, st, n, bv, x1, x0, z, y, rho, lam, h->rhs, h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
         h->launches += 1;
         const int r = read_slots(h, SL_RED, 3);
@@ -914,7 +935,7 @@ int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_o
     int np = 0, r = 0;
     if (h->opt.precision == CSIPM_MIXED) {
         // the FP32 passes of the CG product, on x rounded to FP32
-        convert_kernel<double, float><<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, h->f_p);
+        ew_launch(convert_kernel<double, float>, h->N, h->stream, h->N, x, h->f_p);
         CK(cudaGetLastError());
         CK(cudaMemsetAsync(h->f_Db, 0, sizeof(float) * h->N, h->stream));
         r = profile_impl<float>(h, h->op32, h->f_p, h->f_Db, h->f_q, reps, ms_out, bytes_out, names, &np);

@@ -177,7 +177,7 @@ extern "C" {
 
 int csipm_gondzio_obj(csipm_handle h, const double* x, double* f) {
     if (!h || !x || !f) return fail(h, CSIPM_ERR_INVALID, "null argument");
-    gz_obj_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, h->ws(h->slots + SL_DOT));
+    ew_launch(gz_obj_kernel, h->N, h->stream, h->N, x, h->ws(h->slots + SL_DOT));
     CK(cudaGetLastError());
     const int r = read_slots(h, SL_DOT, 2);
     if (r) return r;
@@ -187,7 +187,7 @@ int csipm_gondzio_obj(csipm_handle h, const double* x, double* f) {
 
 int csipm_gondzio_grad(csipm_handle h, const double* x, double* g) {
     if (!h || !x || !g) return fail(h, CSIPM_ERR_INVALID, "null argument");
-    gz_grad_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, h->lambda, g);
+    ew_launch(gz_grad_kernel, h->N, h->stream, h->N, x, h->lambda, g);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -197,11 +197,10 @@ int csipm_gondzio_cons(csipm_handle h, const double* x, double* c) {
     int r = ensure_gondzio_buffers(h);
     if (r) return r;
     const long long n = h->N;
-    const int nb = ew_blocks(n);
-    gz_diff_kernel<<<nb, EW_THREADS, 0, h->stream>>>(n, x, 1.0, h->gz_t1);
+    ew_launch(gz_diff_kernel, n, h->stream, n, x, 1.0, h->gz_t1);
     CK(cudaGetLastError());
     CK(op_A(h->op64, h->gz_t1, h->gz_t2, h->stream));
-    gz_cons_kernel<<<nb, EW_THREADS, 0, h->stream>>>(n, h->z0, h->gz_t2, x, c);
+    ew_launch(gz_cons_kernel, n, h->stream, n, h->z0, h->gz_t2, x, c);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -210,7 +209,7 @@ int csipm_gondzio_kkt_build(csipm_handle h, const double* pr_diag) {
     if (!h || !pr_diag) return fail(h, CSIPM_ERR_INVALID, "null argument");
     int r = ensure_gondzio_buffers(h);
     if (r) return r;
-    gz_build_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, pr_diag, h->gz_Dp, h->gz_Dq, h->gz_P11,
+    ew_launch(gz_build_kernel, h->N, h->stream, h->N, pr_diag, h->gz_Dp, h->gz_Dq, h->gz_P11,
                                                                    h->gz_P12, h->gz_P22);
     CK(cudaGetLastError());
     return CSIPM_OK;
@@ -220,7 +219,7 @@ int csipm_gondzio_condensed_mul(csipm_handle h, double* y, const double* x, doub
     if (!h || !x || !y) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!h->gz_Dp) return fail(h, CSIPM_ERR_INVALID, "csipm_gondzio_kkt_build must be called first");
     const long long n = h->N;
-    gz_diff_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, x, 1.0, h->gz_t1);
+    ew_launch(gz_diff_kernel, n, h->stream, n, x, 1.0, h->gz_t1);
     CK(cudaGetLastError());
     EpiGzMul ep{x, y, h->gz_Dp, h->gz_Dq, n, alpha, beta};
     CK(op_AtA(h->op64, (const double*)h->gz_t1, ep, nullptr, h->stream));
@@ -231,7 +230,7 @@ int csipm_gondzio_condensed_mul(csipm_handle h, double* y, const double* x, doub
 int csipm_gondzio_precond_mul(csipm_handle h, double* y, const double* x, double alpha, double beta) {
     if (!h || !x || !y) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!h->gz_Dp) return fail(h, CSIPM_ERR_INVALID, "csipm_gondzio_kkt_build must be called first");
-    precond_mul_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, y, x, h->gz_P11, h->gz_P12, h->gz_P22,
+    ew_launch(precond_mul_kernel, h->N, h->stream, h->N, y, x, h->gz_P11, h->gz_P12, h->gz_P22,
                                                                       alpha, beta);
     CK(cudaGetLastError());
     return CSIPM_OK;
@@ -242,13 +241,12 @@ int csipm_gondzio_kkt_mul(csipm_handle h, double* y, const double* x, double alp
     int r = ensure_gondzio_buffers(h);
     if (r) return r;
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     EpiStore<double> st_t{h->gz_t1};
     CK(op_At(h->op64, x + 3 * n, st_t, h->stream));
-    gz_kktmul1_kernel<<<nb, EW_THREADS, 0, h->stream>>>(n, x, h->gz_t1, y, alpha, beta, h->gz_t2);
+    ew_launch(gz_kktmul1_kernel, n, h->stream, n, x, h->gz_t1, y, alpha, beta, h->gz_t2);
     CK(cudaGetLastError());
     CK(op_A(h->op64, h->gz_t2, h->gz_t1, h->stream));
-    gz_kktmul2_kernel<<<nb, EW_THREADS, 0, h->stream>>>(n, x, h->gz_t1, y, alpha, beta);
+    ew_launch(gz_kktmul2_kernel, n, h->stream, n, x, h->gz_t1, y, alpha, beta);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -259,7 +257,7 @@ int csipm_gondzio_jtprod(csipm_handle h, double* y, const double* x) {
     if (r) return r;
     EpiStore<double> st_t{h->gz_t1};
     CK(op_At(h->op64, x, st_t, h->stream));
-    gz_jtprod_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, h->gz_t1, y);
+    ew_launch(gz_jtprod_kernel, h->N, h->stream, h->N, x, h->gz_t1, y);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -268,28 +266,27 @@ int csipm_gondzio_kkt_solve(csipm_handle h, double* w, int* cg_iters) {
     if (!h || !w) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!h->gz_Dp) return fail(h, CSIPM_ERR_INVALID, "csipm_gondzio_kkt_build must be called first");
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
     const double *P11 = pc ? h->gz_P11 : nullptr, *P12 = pc ? h->gz_P12 : nullptr, *P22 = pc ? h->gz_P22 : nullptr;
     cudaEventRecord(h->ev0, st);
-    gz_sum_kernel<<<nb, EW_THREADS, 0, st>>>(n, w, h->gz_t1);
+    ew_launch(gz_sum_kernel, n, st, n, w, h->gz_t1);
     EpiStore<double> st_t{h->gz_t2};
     CK(op_At(h->op64, h->gz_t1, st_t, st));
-    gz_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, w, h->gz_t2, h->k_b);
+    ew_launch(gz_rhs_kernel, n, st, n, w, h->gz_t2, h->k_b);
     CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
-    kcg_init_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->k_b, h->k_x, h->k_r, h->k_p, P11, P12, P22,
+    ew_launch(kcg_init_kernel, n, st, n, h->k_b, h->k_x, h->k_r, h->k_p, P11, P12, P22,
                                               h->ws(h->slots + SL_DUMMY), h->cgs, h->opt.cg_atol, h->opt.cg_rtol);
     CK(cudaGetLastError());
     int chunk = 2, since = 0;
     const int maxit = h->opt.cg_maxit;
     for (int it = 0; it < maxit; ++it) {
-        gz_diff_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->k_p, 1.0, h->gz_t1);
+        ew_launch(gz_diff_kernel, n, st, n, h->k_p, 1.0, h->gz_t1);
         EpiGzCG ep{h->k_p, h->k_q, h->gz_Dp, h->gz_Dq, n, h->ws(&h->cgs->pq), 0.0};
         CK(op_AtA(h->op64, (const double*)h->gz_t1, ep, &h->cgs->done, st));
-        kcg_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, it, h->k_x, h->k_r, h->k_p, h->k_q, P11, P12, P22,
+        ew_launch(kcg_update_kernel, n, st, n, it, h->k_x, h->k_r, h->k_p, h->k_q, P11, P12, P22,
                                                      h->ws(h->slots + SL_DUMMY), h->cgs);
-        kcg_pupdate_kernel<<<nb, EW_THREADS, 0, st>>>(n, it, h->k_r, h->k_p, P11, P12, P22, h->cgs);
+        ew_launch(kcg_pupdate_kernel, n, st, n, it, h->k_r, h->k_p, P11, P12, P22, h->cgs);
         CK(cudaGetLastError());
         if (++since >= chunk || it + 1 == maxit) {
             since = 0;
@@ -302,10 +299,10 @@ int csipm_gondzio_kkt_solve(csipm_handle h, double* w, int* cg_iters) {
     CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     h->matvecs += h->hcgs->iters;
-    gz_setx_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->k_x, w, h->gz_t1);
+    ew_launch(gz_setx_kernel, n, st, n, h->k_x, w, h->gz_t1);
     CK(cudaGetLastError());
     CK(op_A(h->op64, h->gz_t1, h->gz_t2, st));
-    gz_back_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->gz_t2, w);
+    ew_launch(gz_back_kernel, n, st, n, h->gz_t2, w);
     CK(cudaGetLastError());
     cudaEventRecord(h->ev1, st);
     CK(cudaEventSynchronize(h->ev1));

@@ -53,6 +53,18 @@ inline int ew_blocks(long long n) {
     return (int)b;
 }
 
+// Grid of a grid-stride element kernel: exactly one resident wave (the SM
+// count times the EW_THREADS-thread CTAs that fit on an SM with the
+// kernel's registers), or fewer CTAs when n is small.  A fixed grid above
+// one wave leaves a partial second wave: at 40 registers 1184 CTAs are 1.33
+// waves and the kernel streams at half the HBM rate.  Cached per kernel.
+int ew_grid(const void* kernel, long long n);
+
+template <typename... P, typename... A>
+inline void ew_launch(void (*kernel)(P...), long long n, cudaStream_t st, A&&... args) {
+    kernel<<<ew_grid((const void*)kernel, n), EW_THREADS, 0, st>>>(std::forward<A>(args)...);
+}
+
 inline bool valid_dims(int dim, const int* size, std::string* err, int* status) {
     if (dim < 1 || dim > 3 || !size) { *err = "dim must be 1, 2 or 3"; *status = CSIPM_ERR_INVALID; return false; }
     long long N = 1;

@@ -25,11 +25,11 @@ int csipm_obj(csipm_handle h, const double* x, double* f) {
     CK(op_AtA(h->op64, x, ep, nullptr, h->stream));
     h->matvecs++;
     const long long n = h->N;
-    dot2_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, x, h->Qb, x, h->b, h->ws(h->slots + SL_DOT));
+    ew_launch(dot2_kernel, n, h->stream, n, x, h->Qb, x, h->b, h->ws(h->slots + SL_DOT));
     CK(cudaGetLastError());
     // sum(c) = c . 1 : reuse Minv as a ones vector would cost a fill; use a dedicated reduction
-    fill_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, 1.0, h->rhs);
-    dot2_kernel<<<ew_blocks(n), EW_THREADS, 0, h->stream>>>(n, x + n, h->rhs, nullptr, nullptr, h->ws(h->slots + SL_DOT + 2));
+    ew_launch(fill_kernel, n, h->stream, n, 1.0, h->rhs);
+    ew_launch(dot2_kernel, n, h->stream, n, x + n, h->rhs, nullptr, nullptr, h->ws(h->slots + SL_DOT + 2));
     CK(cudaGetLastError());
     int r = read_slots(h, SL_DOT, 3);
     if (r) return r;
@@ -42,14 +42,14 @@ int csipm_grad(csipm_handle h, const double* x, double* g) {
     EpiGrad ep{h->b, g};
     CK(op_AtA(h->op64, x, ep, nullptr, h->stream));
     h->matvecs++;
-    fill_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, h->lambda, g + h->N);
+    ew_launch(fill_kernel, h->N, h->stream, h->N, h->lambda, g + h->N);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
 
 int csipm_cons(csipm_handle h, const double* x, double* c) {
     if (!h || !x || !c) return fail(h, CSIPM_ERR_INVALID, "null argument");
-    cons_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, x, c);
+    ew_launch(cons_kernel, h->N, h->stream, h->N, x, c);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -59,7 +59,7 @@ int csipm_hprod(csipm_handle h, const double* v, double* hv, double obj_weight) 
     EpiScale ep{obj_weight, hv};
     CK(op_AtA(h->op64, v, ep, nullptr, h->stream));
     h->matvecs++;
-    fill_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, 0.0, hv + h->N);
+    ew_launch(fill_kernel, h->N, h->stream, h->N, 0.0, hv + h->N);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -68,7 +68,7 @@ int csipm_kkt_build(csipm_handle h, const double* pr_diag) {
     if (!h || !pr_diag) return fail(h, CSIPM_ERR_INVALID, "null argument");
     int r = ensure_kkt_buffers(h);
     if (r) return r;
-    kkt_build_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, pr_diag, h->L1, h->L2, h->P11, h->P12, h->P22);
+    ew_launch(kkt_build_kernel, h->N, h->stream, h->N, pr_diag, h->L1, h->L2, h->P11, h->P12, h->P22);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -85,7 +85,7 @@ int csipm_condensed_mul(csipm_handle h, double* y, const double* x, double alpha
 int csipm_precond_mul(csipm_handle h, double* y, const double* x, double alpha, double beta) {
     if (!h || !x || !y) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!h->L1) return fail(h, CSIPM_ERR_INVALID, "csipm_kkt_build must be called first");
-    precond_mul_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, y, x, h->P11, h->P12, h->P22, alpha, beta);
+    ew_launch(precond_mul_kernel, h->N, h->stream, h->N, y, x, h->P11, h->P12, h->P22, alpha, beta);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -100,7 +100,7 @@ int csipm_kkt_mul(csipm_handle h, double* y, const double* x, double alpha, doub
 
 int csipm_jtprod(csipm_handle h, double* y, const double* x) {
     if (!h || !x || !y) return fail(h, CSIPM_ERR_INVALID, "null argument");
-    jtprod_kernel<<<ew_blocks(h->N), EW_THREADS, 0, h->stream>>>(h->N, y, x);
+    ew_launch(jtprod_kernel, h->N, h->stream, h->N, y, x);
     CK(cudaGetLastError());
     return CSIPM_OK;
 }
@@ -109,14 +109,13 @@ int csipm_kkt_solve(csipm_handle h, double* w, const double* pr_diag, int* cg_it
     if (!h || !w || !pr_diag) return fail(h, CSIPM_ERR_INVALID, "null argument");
     if (!h->L1) return fail(h, CSIPM_ERR_INVALID, "csipm_kkt_build must be called first");
     const long long n = h->N;
-    const int nb = ew_blocks(n);
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
     const double *P11 = pc ? h->P11 : nullptr, *P12 = pc ? h->P12 : nullptr, *P22 = pc ? h->P22 : nullptr;
     cudaEventRecord(h->ev0, st);
-    kkt_rhs_kernel<<<nb, EW_THREADS, 0, st>>>(n, w, pr_diag, h->k_b);
+    ew_launch(kkt_rhs_kernel, n, st, n, w, pr_diag, h->k_b);
     CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
-    kcg_init_kernel<<<nb, EW_THREADS, 0, st>>>(n, h->k_b, h->k_x, h->k_r, h->k_p, P11, P12, P22,
+    ew_launch(kcg_init_kernel, n, st, n, h->k_b, h->k_x, h->k_r, h->k_p, P11, P12, P22,
                                               h->ws(h->slots + SL_DUMMY), h->cgs, h->opt.cg_atol, h->opt.cg_rtol);
     CK(cudaGetLastError());
     int chunk = 2, since = 0;
@@ -124,9 +123,9 @@ int csipm_kkt_solve(csipm_handle h, double* w, const double* pr_diag, int* cg_it
     for (int it = 0; it < maxit; ++it) {
         EpiKcg ep{h->k_p, h->k_q, h->L1, h->L2, n, h->ws(&h->cgs->pq), 0.0};
         CK(op_AtA(h->op64, h->k_p, ep, &h->cgs->done, st));
-        kcg_update_kernel<<<nb, EW_THREADS, 0, st>>>(n, it, h->k_x, h->k_r, h->k_p, h->k_q, P11, P12, P22,
+        ew_launch(kcg_update_kernel, n, st, n, it, h->k_x, h->k_r, h->k_p, h->k_q, P11, P12, P22,
                                                      h->ws(h->slots + SL_DUMMY), h->cgs);
-        kcg_pupdate_kernel<<<nb, EW_THREADS, 0, st>>>(n, it, h->k_r, h->k_p, P11, P12, P22, h->cgs);
+        ew_launch(kcg_pupdate_kernel, n, st, n, it, h->k_r, h->k_p, P11, P12, P22, h->cgs);
         CK(cudaGetLastError());
         if (++since >= chunk || it + 1 == maxit) {
             since = 0;
@@ -139,7 +138,7 @@ int csipm_kkt_solve(csipm_handle h, double* w, const double* pr_diag, int* cg_it
     CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     h->matvecs += h->hcgs->iters;
-    kkt_back_kernel<<<nb, EW_THREADS, 0, st>>>(n, w, h->k_x, pr_diag);
+    ew_launch(kkt_back_kernel, n, st, n, w, h->k_x, pr_diag);
     CK(cudaGetLastError());
     cudaEventRecord(h->ev1, st);
     CK(cudaEventSynchronize(h->ev1));
