@@ -78,13 +78,24 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
     }
     const double alpha = rz / pq;
     double acc[1] = {0.0};
-    CSIPM_GRID_LOOP(i, n) {
-        const double pv = (double)p[i];
-        x[i] = (TX)((double)x[i] + alpha * pv);
-        const double rv = (double)r[i] - alpha * (double)q[i];
-        r[i] = (TV)rv;
-        acc[0] += Minv ? rv * (double)Minv[i] * rv : rv * rv;
+    auto elem = [&](long long k, double xv, double rv0, double pv, double qv, double mv) {
+        x[k] = (TX)(xv + alpha * pv);
+        const double rv = rv0 - alpha * qv;
+        r[k] = (TV)rv;
+        acc[0] += Minv ? rv * mv * rv : rv * rv;
+    };
+    // two elements per trip with all loads issued first (load latency)
+    const long long G = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + G < n; i += 2 * G) {
+        const long long j = i + G;
+        const double xi = (double)x[i], xj = (double)x[j], ri = (double)r[i], rj = (double)r[j];
+        const double pi = (double)p[i], pj = (double)p[j], qi = (double)q[i], qj = (double)q[j];
+        const double mi = Minv ? (double)Minv[i] : 1.0, mj = Minv ? (double)Minv[j] : 1.0;
+        elem(i, xi, ri, pi, qi, mi);
+        elem(j, xj, rj, pj, qj, mj);
     }
+    if (i < n) elem(i, (double)x[i], (double)r[i], (double)p[i], (double)q[i], Minv ? (double)Minv[i] : 1.0);
     if (grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) {
         const double rzn = ws.out[0];
         sc->rz[(it + 1) & 1] = rzn;
@@ -100,10 +111,16 @@ static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restri
                                   const CgScalars* sc) {
     if (sc->done) return;
     const double b = sc->rz[(it + 1) & 1] / sc->rz[it & 1];
-    CSIPM_GRID_LOOP(i, n) {
-        const double zv = Minv ? (double)Minv[i] * (double)r[i] : (double)r[i];
-        p[i] = (TV)(zv + b * (double)p[i]);
+    const long long G = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + G < n; i += 2 * G) {
+        const long long j = i + G;
+        const double ri = (double)r[i], rj = (double)r[j], pi = (double)p[i], pj = (double)p[j];
+        const double mi = Minv ? (double)Minv[i] : 1.0, mj = Minv ? (double)Minv[j] : 1.0;
+        p[i] = (TV)(mi * ri + b * pi);
+        p[j] = (TV)(mj * rj + b * pj);
     }
+    if (i < n) p[i] = (TV)((Minv ? (double)Minv[i] : 1.0) * (double)r[i] + b * (double)p[i]);
 }
 
 // Mixed precision: r = rhs - q in FP64 with r.(Minv r) (the refinement residual)
@@ -263,22 +280,21 @@ struct MinRatio {
     __device__ __forceinline__ double value() const { return den > 0.0 ? num / den : DBL_MAX; }
 };
 
-static __global__ void ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+static __global__ void __launch_bounds__(EW_THREADS, 3) ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                      const double* __restrict__ z1, const double* __restrict__ z2,
                                      const double* __restrict__ dba, const double* __restrict__ sigmu_p,
                                      const double* __restrict__ db, RedWorkspace ws) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
     MinRatio mp, md;
-    CSIPM_GRID_LOOP(i, n) {
-        const double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
+    auto elem = [&](double s1, double s2, double a, double d, double xa, double x) {
         const ElemPre e = elem_pre(s1, s2, a, d);
         ElemDir o;
         if (dba) {
-            const ElemDir f = elem_affine(e, lam, dba[i]);
-            o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, db[i]);
+            const ElemDir f = elem_affine(e, lam, xa);
+            o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, x);
         } else {
-            o = elem_affine(e, lam, db[i]);
+            o = elem_affine(e, lam, x);
         }
         if (o.ds1 < 0.0) mp.add(s1, -o.ds1);
         if (o.ds2 < 0.0) mp.add(s2, -o.ds2);
@@ -287,7 +303,21 @@ static __global__ void ipm_stepstats_kernel(long long n, double lam, const doubl
         acc[SS_SZ] += s1 * a + s2 * d;
         acc[SS_CROSS] += s1 * o.dz1 + o.ds1 * a + s2 * o.dz2 + o.ds2 * d;
         acc[SS_DD] += o.ds1 * o.dz1 + o.ds2 * o.dz2;
+    };
+    // two elements per trip, all their loads issued before the FP64 math
+    // (the kernel is otherwise bound by load latency at its occupancy)
+    const long long G = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + G < n; i += 2 * G) {
+        const long long j = i + G;
+        const double s1i = s1v[i], s1j = s1v[j], s2i = s2v[i], s2j = s2v[j];
+        const double ai = z1[i], aj = z1[j], di = z2[i], dj = z2[j];
+        const double xai = dba ? dba[i] : 0.0, xaj = dba ? dba[j] : 0.0;
+        const double xi = db[i], xj = db[j];
+        elem(s1i, s2i, ai, di, xai, xi);
+        elem(s1j, s2j, aj, dj, xaj, xj);
     }
+    if (i < n) elem(s1v[i], s2v[i], z1[i], z2[i], dba ? dba[i] : 0.0, db[i]);
     acc[SS_MINP] = mp.value();
     acc[SS_MIND] = md.value();
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
@@ -354,25 +384,24 @@ static __global__ void admm_update_kernel(long long n, const double* __restrict_
 // precision), and the predictor right-hand side (h1 = -z1, h2 = -z2,
 // fc = -lambda).
 template <typename TV>
-static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb,
-                                          double lam, const double* __restrict__ beta, double* __restrict__ s1v,
-                                          double* __restrict__ s2v, double* __restrict__ z1,
-                                          double* __restrict__ z2, const double* __restrict__ dba,
-                                          const double* __restrict__ db, const double* __restrict__ sigmu_p,
-                                          const double* __restrict__ alpha_p, double* __restrict__ rd,
-                                          double* __restrict__ Db, double* __restrict__ Minv, TV* __restrict__ Db_lo,
-                                          TV* __restrict__ Minv_lo, int precond, double* __restrict__ rhs,
-                                          RedWorkspace ws) {
+static __global__ void __launch_bounds__(EW_THREADS, 3)
+ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+                   const double* __restrict__ beta, double* __restrict__ s1v, double* __restrict__ s2v,
+                   double* __restrict__ z1, double* __restrict__ z2, const double* __restrict__ dba,
+                   const double* __restrict__ db, const double* __restrict__ sigmu_p,
+                   const double* __restrict__ alpha_p, double* __restrict__ rd, double* __restrict__ Db,
+                   double* __restrict__ Minv, TV* __restrict__ Db_lo, TV* __restrict__ Minv_lo, int precond,
+                   double* __restrict__ rhs, RedWorkspace ws) {
     double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
     const bool step = db != nullptr;
     const double sigmu = step ? *sigmu_p : 0.0;
     const double alpha = step ? *alpha_p : 0.0;
-    CSIPM_GRID_LOOP(i, n) {
-        double s1 = s1v[i], s2 = s2v[i], a = z1[i], d = z2[i];
+    auto elem = [&](long long i, double s1, double s2, double a, double d, double xa, double x, double be, double q,
+                    double bb) {
         if (step) {
             const ElemPre e = elem_pre(s1, s2, a, d);
-            const ElemDir f = elem_affine(e, lam, dba[i]);
-            const ElemDir o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, db[i]);
+            const ElemDir f = elem_affine(e, lam, xa);
+            const ElemDir o = elem_dir(e, lam, sigmu, f.ds1 * f.dz1, f.ds2 * f.dz2, x);
             s1 += alpha * o.ds1;
             s2 += alpha * o.ds2;
             a += alpha * o.dz1;
@@ -382,7 +411,6 @@ static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict_
             z1[i] = a;
             z2[i] = d;
         }
-        const double be = beta[i], q = Qb[i], bb = b[i];
         const double ce = 0.5 * (s1 + s2);
         const double r = q - bb - a + d;
         rd[i] = r;
@@ -402,7 +430,22 @@ static __global__ void ipm_resdiag_kernel(long long n, const double* __restrict_
         if (Db) { Db[i] = dbv; Minv[i] = mi; }
         if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
         rhs[i] = -r - a + d + L2 * lam * iL1;
+    };
+    // two elements per trip with all loads issued first (load latency)
+    const long long G = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + G < n; i += 2 * G) {
+        const long long j = i + G;
+        const double s1i = s1v[i], s1j = s1v[j], s2i = s2v[i], s2j = s2v[j];
+        const double ai = z1[i], aj = z1[j], di = z2[i], dj = z2[j];
+        const double xai = step ? dba[i] : 0.0, xaj = step ? dba[j] : 0.0;
+        const double xi = step ? db[i] : 0.0, xj = step ? db[j] : 0.0;
+        const double bei = beta[i], bej = beta[j], qi = Qb[i], qj = Qb[j], bbi = b[i], bbj = b[j];
+        elem(i, s1i, s2i, ai, di, xai, xi, bei, qi, bbi);
+        elem(j, s1j, s2j, aj, dj, xaj, xj, bej, qj, bbj);
     }
+    if (i < n)
+        elem(i, s1v[i], s2v[i], z1[i], z2[i], step ? dba[i] : 0.0, step ? db[i] : 0.0, beta[i], Qb[i], b[i]);
     grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
 }
 
