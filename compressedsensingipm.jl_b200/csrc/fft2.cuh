@@ -228,19 +228,34 @@ strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
 }
 
 // ---------------------------------------------------------------- row pass
+// Rows per CTA of the row pass: as many as fit in 48 KB of static shared
+// memory, at most 8 (16-row CTAs of 256 threads measured 12% slower at
+// M = 160 on B200, though they fill whole warps in both mappings).
+constexpr int row2_rows(int per_row_bytes) {
+    const int r0 = (48 * 1024) / per_row_bytes;
+    return r0 > 8 ? 8 : (r0 < 1 ? 1 : r0);
+}
+
 // M = A*B half-spectrum length (dim-1 complex FFT length); rows of M+1 values.
 template <typename T, int A, int B> struct Row2Shape {
     static constexpr int M = A * B;
     static constexpr int X1 = A * (B + 1);          // inverse exchange  [ka][t],  t-stride 1, ka-stride B+1
     static constexpr int X2 = B * (A + 1);          // forward exchange  [kb][s],  s-stride 1, kb-stride A+1
     static constexpr int XC = X1 > X2 ? X1 : X2;
-    static constexpr int PER_ROW = XC + M + 1;      // exchange area + natural-order spectrum for R2C post
-    // rows per CTA: as many as fit in 48 KB of static shared memory, at most 8
-    static constexpr int R0 = (48 * 1024) / (PER_ROW * (int)sizeof(cplx_t<T>));
-    static constexpr int ROWS = R0 > 8 ? 8 : (R0 < 1 ? 1 : R0);
+    static constexpr int BASE = XC + M + 1;         // exchange area + natural-order spectrum for R2C post
+    // row pitch = A (mod 16) complex: in the A-task phases a half-warp spans
+    // two rows, and the next row's lanes then land on the banks after the
+    // first row's (8-byte complex: 16 bank pairs; 16-byte: 8 bank quads)
+    static constexpr int PER_ROW = BASE + (((A - BASE) % 16) + 16) % 16;
     static constexpr int NTL = A > B ? A : B;
+    static constexpr int ROWS = row2_rows(PER_ROW * (int)sizeof(cplx_t<T>));
 };
 
+// Two thread mappings share the CTA: the B-task phases (inverse step 1,
+// forward step 2, C2R/R2C pre/post-processing) give each row NTL = B
+// consecutive threads; the A-task phases (inverse step 2, scale + mask,
+// forward step 1: the B-point DFTs) give each row A consecutive threads, so
+// ROWS*A threads work in whole warps instead of A of every B lanes.
 template <typename T, int A, int B, int IN, int OUT, bool MASK>
 __global__ void __launch_bounds__(Row2Shape<T, A, B>::ROWS * Row2Shape<T, A, B>::NTL)
 row2_kernel(PassArgs<T> a) {
@@ -248,30 +263,38 @@ row2_kernel(PassArgs<T> a) {
     using Sh = Row2Shape<T, A, B>;
     constexpr int M = Sh::M;
     constexpr int NTL = Sh::NTL;
+    static_assert(A <= B, "row pass factors are ordered A <= B");
     if (a.skip && *a.skip) return;
     __shared__ C S[Sh::ROWS * Sh::PER_ROW];
+    // B-task mapping
     const int r = threadIdx.x / NTL, t = threadIdx.x % NTL;
     const int row = blockIdx.x * Sh::ROWS + r;
     const bool live = row < a.nrows;
     C* X = S + r * Sh::PER_ROW;           // exchange area of this row
     C* P = X + Sh::XC;                    // natural-order spectrum (R2C post)
+    // A-task mapping
+    const bool ta = threadIdx.x < Sh::ROWS * A;
+    const int ra = threadIdx.x / A, s = threadIdx.x % A;
+    const int rowa = blockIdx.x * Sh::ROWS + ra;
+    const bool livea = ta && rowa < a.nrows;
+    C* XA = S + (ta ? ra : 0) * Sh::PER_ROW;
     const C* __restrict__ tw = a.tw;      // N1-th roots, W_M^e = tw[2e]
     const C zero = mk((T)0, (T)0);
     const T sc = (T)a.scale;
 
-    // z[s + A*kb] for the thread s < A after the inverse transform (or the load)
+    // z[s + A*kb] of the A-task s after the inverse transform (or the load)
     C z[B];
     if (IN == IN_REAL) {
-        if (t < A) {
+        if (ta) {
 #pragma unroll
             for (int kb = 0; kb < B; ++kb) {
-                const int n = t + A * kb;
-                z[kb] = live ? *reinterpret_cast<const C*>(a.real_in + (size_t)row * a.g.n1 + 2 * n) : zero;
+                const int n = s + A * kb;
+                z[kb] = livea ? *reinterpret_cast<const C*>(a.real_in + (size_t)rowa * a.g.n1 + 2 * n) : zero;
             }
         }
     } else {
-        // ---- inverse step 1 (thread t < B): C2R pre-processing at load
-        if (t < B) {
+        // ---- inverse step 1 (B-task t): C2R pre-processing at load
+        {
             C v[A];
             const C* rowp = a.spec + (size_t)row * a.g.ld1;
 #pragma unroll
@@ -294,47 +317,47 @@ row2_kernel(PassArgs<T> a) {
             }
         }
         __syncthreads();
-        // ---- inverse step 2 (thread s < A)
-        if (t < A) {
+        // ---- inverse step 2 (A-task s)
+        if (ta) {
 #pragma unroll
-            for (int q = 0; q < B; ++q) z[q] = X[t * (B + 1) + q];
+            for (int q = 0; q < B; ++q) z[q] = XA[s * (B + 1) + q];
             Dft<B, true, T>::run(z);
         }
-        __syncthreads();   // X is reused by the forward exchange
+        __syncthreads();   // the exchange area is reused by the forward transform
     }
     // ---- scale and mask the real samples (x[2n], x[2n+1]) = z[n], n = s + A*kb
-    if (t < A) {
+    if (ta) {
 #pragma unroll
         for (int kb = 0; kb < B; ++kb) {
-            const int n = t + A * kb;
+            const int n = s + A * kb;
             C y = z[kb];
             y.x *= sc;
             y.y *= sc;
-            if (MASK && live) {
-                const uint32_t w = a.maskw[(size_t)row * a.wpr + (n >> 4)];
+            if (MASK && livea) {
+                const uint32_t w = a.maskw[(size_t)rowa * a.wpr + (n >> 4)];
                 const int sh = (2 * n) & 31;
                 if (!((w >> sh) & 1u)) y.x = (T)0;
                 if (!((w >> (sh + 1)) & 1u)) y.y = (T)0;
             }
             z[kb] = y;
-            if (OUT == OUT_REAL && live) *reinterpret_cast<C*>(a.real_out + (size_t)row * a.g.n1 + 2 * n) = y;
+            if (OUT == OUT_REAL && livea) *reinterpret_cast<C*>(a.real_out + (size_t)rowa * a.g.n1 + 2 * n) = y;
         }
     }
     if (OUT == OUT_REAL) return;
-    // ---- forward transform with factors (B, A): step 1 on the thread's own z
-    if (t < A) {
+    // ---- forward transform with factors (B, A): step 1 (A-task s) on its own z
+    if (ta) {
         Dft<B, false, T>::run(z);
 #pragma unroll
         for (int kb = 0; kb < B; ++kb) {
             C w = z[kb];
-            const int e = t * kb;
+            const int e = s * kb;
             if (e) w = cmul(w, tw[2 * e]);
-            X[kb * (A + 1) + t] = w;
+            XA[kb * (A + 1) + s] = w;
         }
     }
     __syncthreads();
-    // step 2 (thread t < B): outputs Z[t + B*ka]
-    if (t < B) {
+    // step 2 (B-task t): outputs Z[t + B*ka]
+    {
         C u[A];
 #pragma unroll
         for (int q = 0; q < A; ++q) u[q] = X[t * (A + 1) + q];
