@@ -294,7 +294,7 @@ static void ensure_diag64(csipm_handle h) {
 }
 
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v) {
+                const double* r0v, float* xf) {
     const long long n = h->N;
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
@@ -309,11 +309,26 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
     const bool given = has_x0 && r0v != nullptr;
     const bool fp32_warm = has_x0 && !given && rtol >= MIXED_FP32_WARM_RTOL;
     h->resid_kind = RESID_NONE;
-    if (!has_x0) CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    // with xf, round 0 iterates on xf itself (no correction vector, no FP64
+    // accumulation); any FP64 step (refinement, fallback) first takes the
+    // iterate into x, and the result goes back to xf at the end
+    bool in32 = xf != nullptr;
+    auto to64 = [&]() {
+        if (!in32) return;
+        ew_launch(convert_kernel<float, double>, n, st, n, (const float*)xf, x);
+        h->launches += 1;
+        in32 = false;
+    };
+    if (!has_x0) {
+        if (in32) CK(cudaMemsetAsync(xf, 0, sizeof(float) * n, st));
+        else CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    }
+    int status = CSIPM_OK;
     for (int round = 0;; ++round) {
         const double* res = given && round == 0 ? r0v : rhs;
         double rin = std::max(rtol, MIXED_INNER_RTOL);
         if (round > 0 || (has_x0 && !fp32_warm && !given)) {
+            to64();
             ensure_diag64(h);
             EpiCG<double> ep{x, h->Db, h->cg_q, h->ws(h->slots + SL_DUMMY), 0.0};
             CK(solve_AtA(h, x, ep, nullptr, st));
@@ -337,14 +352,19 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             }
             res = h->cg_r;
         }
-        // FP32 PCG from d = 0 on K d = res
+        // FP32 PCG on K d = res: from d = 0 into f_x, or (in32) on xf from its start
+        float* xi = in32 ? xf : h->f_x;
         CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
-        CK(cudaMemsetAsync(h->f_x, 0, sizeof(float) * n, st));
+        if (!in32) CK(cudaMemsetAsync(h->f_x, 0, sizeof(float) * n, st));
         if (round == 0 && fp32_warm) {
             // warm-start residual rhs - K x0 with the FP32 product (x0 rounded to FP32)
-            ew_launch(convert_kernel<double, float>, n, st, n, x, h->f_p);
-            EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(h->slots + SL_DUMMY), 0.0};
-            CK(solve_AtA32(h, h->f_p, ep, nullptr, st));
+            const float* x0f = xf;
+            if (!in32) {
+                ew_launch(convert_kernel<double, float>, n, st, n, (const double*)x, h->f_p);
+                x0f = h->f_p;
+            }
+            EpiCG<float> ep{x0f, h->f_Db, h->f_q, h->ws(h->slots + SL_DUMMY), 0.0};
+            CK(solve_AtA32(h, x0f, ep, nullptr, st));
             h->matvecs++;
             h->launches += ppp + 1;
             ew_launch(cg_init_kernel<float>, n, st, n, rhs, h->f_q, 1, Minv32, h->f_r, h->f_p,
@@ -360,13 +380,16 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
             cudaError_t e = solve_AtA32(h, h->f_p, ep, &h->cgs->done, s);
             if (e != cudaSuccess) return e;
-            ew_launch(cg_update_kernel<float, float>, n, s, n, it, h->f_x, h->f_r, h->f_p, h->f_q, Minv32,
+            ew_launch(cg_update_kernel<float, float>, n, s, n, it, xi, h->f_r, h->f_p, h->f_q, Minv32,
                                                                     h->ws(h->slots + SL_DUMMY), h->cgs);
             ew_launch(cg_pupdate_kernel<float>, n, s, n, it, h->f_r, Minv32, h->f_p, h->cgs);
             return cudaGetLastError();
         };
         {
-            const int r = cg_iterations(h, &h->cg_exec32, cap, iteration, ppp + 2);
+            // a graph holds its vectors: one per iterate buffer
+            cudaGraphExec_t* ex = xi == h->f_x ? &h->cg_exec32[0]
+                                  : (xi == h->f_dba ? &h->cg_exec32[1] : (xi == h->f_db ? &h->cg_exec32[2] : nullptr));
+            const int r = cg_iterations(h, ex, cap, iteration, ppp + 2);
             if (r) return r;
         }
         CK(cudaMemcpyAsync(h->hcgs, h->cgs, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
@@ -374,25 +397,32 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         h->matvecs += h->hcgs->iters;
         total += h->hcgs->iters;
         if (r0 < 0.0) r0 = rn = std::sqrt(h->hcgs->rz0);   // |rhs| in the M-norm
-        ew_launch(add_f32_kernel, n, st, n, h->f_x, x);
-        CK(cudaGetLastError());
-        h->launches += 1;
+        if (!in32) {
+            ew_launch(add_f32_kernel, n, st, n, h->f_x, x);
+            CK(cudaGetLastError());
+            h->launches += 1;
+        }
         if (h->hcgs->breakdown) {
+            to64();
             ensure_diag64(h);
             int its = 0;
-            const int r = schur_cg(h, rhs, x, true, std::min(0.5, rtol * r0 / rn), maxit, &its);
+            status = schur_cg(h, rhs, x, true, std::min(0.5, rtol * r0 / rn), maxit, &its);
             total += its;
             h->fallbacks++;
-            *iters = total;
-            return r;
+            break;
         }
         if (rtol >= MIXED_INNER_RTOL && round == 0 && h->hcgs->done) {
             h->resid_kind = RESID_F32;   // f_r = res - K32 d with x = x0 + d
             break;
         }
     }
+    if (xf && !in32) {
+        ew_launch(convert_kernel<double, float>, n, st, n, (const double*)x, xf);
+        CK(cudaGetLastError());
+        h->launches += 1;
+    }
     *iters = total;
-    return CSIPM_OK;
+    return status;
 }
 
 // Times each pass of one A^T A product (the CG product: gather -> ... ->
@@ -589,7 +619,8 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         !h->alloc(&h->db, n_) || !h->alloc(&h->cg_r, n_) || !h->alloc(&h->cg_p, n_) || !h->alloc(&h->cg_q, n_))
         return bail(CSIPM_ERR_OOM, h->err);
     if (mixed && (!h->alloc(&h->f_Db, n_) || !h->alloc(&h->f_Minv, n_) || !h->alloc(&h->f_r, n_) ||
-                  !h->alloc(&h->f_p, n_) || !h->alloc(&h->f_q, n_) || !h->alloc(&h->f_x, n_)))
+                  !h->alloc(&h->f_p, n_) || !h->alloc(&h->f_q, n_) || !h->alloc(&h->f_x, n_) ||
+                  !h->alloc(&h->f_dba, n_) || !h->alloc(&h->f_db, n_)))
         return bail(CSIPM_ERR_OOM, h->err);
     static_assert(sizeof(double) * SL_COUNT == csipm_handle_s::HSLOT_BYTES, "slot block size");
     static_assert(sizeof(CgScalars) <= csipm_handle_s::HCGS_BYTES, "CG scalar block size");
@@ -712,6 +743,10 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     // mixed precision with a Newton tolerance the FP32 warm start serves:
     // the FP64 barrier diagonals are only computed when a solve needs them
     const bool lazy64 = mixed && o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL;
+    // the same loose mode keeps the Newton directions in FP32 (f_dba, f_db):
+    // they are only asked to a relative accuracy >= 1e-4, far above FP32
+    // rounding, and the IPM residual is recomputed in FP64 every iteration
+    const bool dir32 = lazy64;
     cudaEventRecord(h->ev0, st);
     // every beta-space vector of the solve is in solver order when h->sorder
     const double* bv = h->sorder ? h->bs : h->b;
@@ -745,11 +780,17 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         h->launches += 1;   // pending s/z step + residual + barrier diagonals + predictor right-hand side
         const bool step = k > 0;
         h->diag64_stale = lazy64;
-        ew_launch(ipm_resdiag_kernel<float>, n, st, 
-            n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2, step ? h->dba : nullptr, step ? h->db : nullptr,
-            h->slots + SL_SIGMU, h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
-            mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
-            h->ws(h->slots + SL_RED));
+        if (dir32)
+            ew_launch(ipm_resdiag_kernel<float, float>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
+                      step ? h->f_dba : nullptr, step ? h->f_db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
+                      h->rd, (double*)nullptr, (double*)nullptr, h->f_Db, h->f_Minv, o.preconditioner, h->rhs,
+                      h->ws(h->slots + SL_RED));
+        else
+            ew_launch(ipm_resdiag_kernel<float, double>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1,
+                      h->z2, step ? h->dba : nullptr, step ? h->db : nullptr, h->slots + SL_SIGMU,
+                      h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
+                      mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
+                      h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
         int r = read_slots(h, SL_RED, RR_N);
         if (r) return r;
@@ -776,7 +817,8 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         if (k >= o.max_iter) { status = CSIPM_ERR_IPM_MAXITER; break; }
         // ---- predictor (affine scaling): diagonals and right-hand side came with the residual
         int its = 0;
-        int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its)
+        int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its, nullptr,
+                                     dir32 ? h->f_dba : nullptr)
                        : schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
@@ -784,8 +826,12 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         // from the step statistics: no host round trip inside the iteration
         double* sigmu_d = h->slots + SL_SIGMU;
         double* alpha_d = h->slots + SL_ALPHA;
-        ew_launch(ipm_stepstats_kernel, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, nullptr, nullptr, h->dba,
-                                                        h->ws(h->slots + SL_SS));
+        if (dir32)
+            ew_launch(ipm_stepstats_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, (const float*)nullptr,
+                      (const double*)nullptr, h->f_dba, h->ws(h->slots + SL_SS));
+        else
+            ew_launch(ipm_stepstats_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
+                      (const double*)nullptr, (const double*)nullptr, h->dba, h->ws(h->slots + SL_SS));
         ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, mu, 2.0 * (double)n, sigmu_d);
         // ---- corrector, warm-started at dba.  Its starting residual
         // rhs_c - K dba = rhs_c - rhs_p + (rhs_p - K dba) comes from the
@@ -793,25 +839,40 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         // product; mixed precision at tight Newton tolerances computes it
         // with an FP64 product instead, as refinement wants.
         const int rk = (!mixed || o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL) ? h->resid_kind : RESID_NONE;
-        if (rk == RESID_F32)
-            ew_launch(ipm_rhs_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
-                                                             sigmu_d, h->rhs, h->f_r, h->db);
+        const float* rp32 = rk == RESID_F32 ? h->f_r : nullptr;
+        const double* rp64 = rk == RESID_CG64 ? h->cg_r : nullptr;
+        if (dir32 && rp32)
+            ew_launch(ipm_rhs_kernel<float, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp32, h->f_db);
+        else if (dir32)
+            ew_launch(ipm_rhs_kernel<double, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp64, h->f_db);
+        else if (rp32)
+            ew_launch(ipm_rhs_kernel<float, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp32, h->db);
         else
-            ew_launch(ipm_rhs_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd, h->dba,
-                                                              sigmu_d, h->rhs, rk == RESID_CG64 ? h->cg_r : nullptr,
-                                                              h->db);
+            ew_launch(ipm_rhs_kernel<double, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp64, h->db);
         CK(cudaGetLastError());
         const double* r0v = rk != RESID_NONE ? h->rd : nullptr;
-        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v)
+        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v,
+                                 dir32 ? h->f_db : nullptr)
                    : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        ew_launch(ipm_stepstats_kernel, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->dba, sigmu_d, h->db,
-                                                        h->ws(h->slots + SL_SS));
+        if (dir32)
+            ew_launch(ipm_stepstats_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
+                      (const float*)h->f_dba, (const double*)sigmu_d, (const float*)h->f_db, h->ws(h->slots + SL_SS));
+        else
+            ew_launch(ipm_stepstats_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
+                      (const double*)h->dba, (const double*)sigmu_d, (const double*)h->db, h->ws(h->slots + SL_SS));
         ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, std::max(0.99, 1.0 - mu), alpha_d);
         // beta steps now (the next A'A product needs it); s and z take the
         // same step inside the next residual pass
-        ew_launch(ipm_beta_step_kernel, n, st, n, h->beta, h->db, alpha_d);
+        if (dir32)
+            ew_launch(ipm_beta_step_kernel<float>, n, st, n, h->beta, (const float*)h->f_db, (const double*)alpha_d);
+        else
+            ew_launch(ipm_beta_step_kernel<double>, n, st, n, h->beta, (const double*)h->db, (const double*)alpha_d);
         CK(cudaGetLastError());
         h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, beta step (+ the Newton solves' launches)
     }

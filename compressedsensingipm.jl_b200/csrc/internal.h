@@ -127,11 +127,13 @@ struct csipm_handle_s {
     const double* z0 = nullptr;     // the caller's z0 (FFTParameters.z0: outlives the handle)
     // mixed precision: FP32 copies of the Schur diagonal / preconditioner and the FP32 CG vectors
     float *f_Db = nullptr, *f_Minv = nullptr, *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_x = nullptr;
+    // FP32 Newton directions (affine, corrector) of loose mixed-precision solves
+    float *f_dba = nullptr, *f_db = nullptr;
     int refinements = 0;
-    // CUDA graphs of the whole CG loop (a conditional while node; FP64: one
-    // per solution vector, dba and db; FP32: one), captured on first use
+    // CUDA graphs of the whole CG loop (a conditional while node), one per
+    // iterate vector (FP64: dba, db; FP32: f_x, f_dba, f_db), captured on first use
     cudaGraphExec_t cg_exec64[2] = {nullptr, nullptr};
-    cudaGraphExec_t cg_exec32 = nullptr;
+    cudaGraphExec_t cg_exec32[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
     bool graphs_off = false;        // a capture failed: plain launches
     bool diag64_stale = false;      // FP64 Db/Minv not yet computed for this iterate (mixed precision)
@@ -151,7 +153,8 @@ struct csipm_handle_s {
     ~csipm_handle_s() {
         for (auto& g : cg_exec64)
             if (g) cudaGraphExecDestroy(g);
-        if (cg_exec32) cudaGraphExecDestroy(cg_exec32);
+        for (auto& g : cg_exec32)
+            if (g) cudaGraphExecDestroy(g);
         for (auto& g : admm_exec)
             if (g) cudaGraphExecDestroy(g);
         for (void* p : allocs) cudaFreeAsync(p, stream);
@@ -378,12 +381,14 @@ enum { RESID_NONE = 0, RESID_CG64 = 1, RESID_F32 = 2 };   // none / FP64 in cg_r
 
 // Newton solves of the condensed system K x = rhs.  has_x0: x holds a start;
 // r0v (optional, with has_x0): rhs - K x0 is already known and no product
-// is spent on it.  On return h->resid_kind says where the residual
+// is spent on it.  xf (schur_mixed, optional): the start and the result are
+// held in FP32 there instead of x (x is then scratch).  On return
+// h->resid_kind says where the residual
 // rhs - K x of the result is held (RESID_*).
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
              const double* r0v = nullptr);
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v = nullptr);
+                const double* r0v = nullptr, float* xf = nullptr);
 int ensure_kkt_buffers(csipm_handle h);
 int ensure_gondzio_buffers(csipm_handle h);
 

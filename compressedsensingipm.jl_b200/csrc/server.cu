@@ -65,7 +65,7 @@ size_t footprint_bytes(int dim, const int* size, int precision, int64_t n_missin
     size_t b = 0;
     b += 24 * 8 * N;                              // FP64 beta-space vectors (IPM state, CG, solver-order A^T z0)
     b += 16 * Nh;                                 // FP64 spectrum
-    if (precision == CSIPM_MIXED) b += 6 * 4 * N + 8 * Nh;   // FP32 CG vectors + FP32 spectrum
+    if (precision == CSIPM_MIXED) b += 8 * 4 * N + 8 * Nh;   // FP32 CG vectors and directions + FP32 spectrum
     if (n_missing > 0) b += (size_t)((n1 + 31) / 32) * 4 * (size_t)(n2 * n3) * (precision == CSIPM_MIXED ? 2 : 1);
     b += 2 * 16 * (size_t)(n2 * n3);              // plane map
     b += 8 * 8 * 65536 + (1 << 20);               // reduction partials, slots, twiddles (upper bound)

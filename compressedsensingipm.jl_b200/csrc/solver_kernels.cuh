@@ -241,17 +241,17 @@ __device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, dou
 // residual rhs - K dba = rhs - rhs_p + rp replaces rd (rd is not needed after
 // this pass; rhs still holds rhs_p on entry); with x0 the warm start
 // x0 = dba is written as well.
-template <typename TR>
+template <typename TR, typename TD>
 static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
-                               const double* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
-                               const TR* __restrict__ rp, double* __restrict__ x0) {
+                               const TD* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
+                               const TR* __restrict__ rp, TD* __restrict__ x0) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     CSIPM_GRID_LOOP(i, n) {
         const ElemPre e = elem_pre(s1v[i], s2v[i], z1[i], z2[i]);
         double cor1 = 0.0, cor2 = 0.0;
         if (dba) {
-            const ElemDir f = elem_affine(e, lam, dba[i]);
+            const ElemDir f = elem_affine(e, lam, (double)dba[i]);
             cor1 = f.ds1 * f.dz1;
             cor2 = f.ds2 * f.dz2;
         }
@@ -280,10 +280,12 @@ struct MinRatio {
     __device__ __forceinline__ double value() const { return den > 0.0 ? num / den : DBL_MAX; }
 };
 
-static __global__ void __launch_bounds__(EW_THREADS, 3) ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
-                                     const double* __restrict__ z1, const double* __restrict__ z2,
-                                     const double* __restrict__ dba, const double* __restrict__ sigmu_p,
-                                     const double* __restrict__ db, RedWorkspace ws) {
+// TD: type the Newton directions are stored in (FP32 in loose mixed precision)
+template <typename TD>
+static __global__ void __launch_bounds__(EW_THREADS, 3)
+ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+                     const double* __restrict__ z1, const double* __restrict__ z2, const TD* __restrict__ dba,
+                     const double* __restrict__ sigmu_p, const TD* __restrict__ db, RedWorkspace ws) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     double acc[SS_N] = {DBL_MAX, DBL_MAX, 0.0, 0.0, 0.0};
     MinRatio mp, md;
@@ -312,12 +314,12 @@ static __global__ void __launch_bounds__(EW_THREADS, 3) ipm_stepstats_kernel(lon
         const long long j = i + G;
         const double s1i = s1v[i], s1j = s1v[j], s2i = s2v[i], s2j = s2v[j];
         const double ai = z1[i], aj = z1[j], di = z2[i], dj = z2[j];
-        const double xai = dba ? dba[i] : 0.0, xaj = dba ? dba[j] : 0.0;
-        const double xi = db[i], xj = db[j];
+        const double xai = dba ? (double)dba[i] : 0.0, xaj = dba ? (double)dba[j] : 0.0;
+        const double xi = (double)db[i], xj = (double)db[j];
         elem(s1i, s2i, ai, di, xai, xi);
         elem(s1j, s2j, aj, dj, xaj, xj);
     }
-    if (i < n) elem(s1v[i], s2v[i], z1[i], z2[i], dba ? dba[i] : 0.0, db[i]);
+    if (i < n) elem(s1v[i], s2v[i], z1[i], z2[i], dba ? (double)dba[i] : 0.0, (double)db[i]);
     acc[SS_MINP] = mp.value();
     acc[SS_MIND] = md.value();
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
@@ -383,12 +385,12 @@ static __global__ void admm_update_kernel(long long n, const double* __restrict_
 // Minv = 1/(1 + Db) (FP64 when Db is given, FP32 copies for mixed
 // precision), and the predictor right-hand side (h1 = -z1, h2 = -z2,
 // fc = -lambda).
-template <typename TV>
+template <typename TV, typename TD>
 static __global__ void __launch_bounds__(EW_THREADS, 3)
 ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                    const double* __restrict__ beta, double* __restrict__ s1v, double* __restrict__ s2v,
-                   double* __restrict__ z1, double* __restrict__ z2, const double* __restrict__ dba,
-                   const double* __restrict__ db, const double* __restrict__ sigmu_p,
+                   double* __restrict__ z1, double* __restrict__ z2, const TD* __restrict__ dba,
+                   const TD* __restrict__ db, const double* __restrict__ sigmu_p,
                    const double* __restrict__ alpha_p, double* __restrict__ rd, double* __restrict__ Db,
                    double* __restrict__ Minv, TV* __restrict__ Db_lo, TV* __restrict__ Minv_lo, int precond,
                    double* __restrict__ rhs, RedWorkspace ws) {
@@ -438,14 +440,15 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
         const long long j = i + G;
         const double s1i = s1v[i], s1j = s1v[j], s2i = s2v[i], s2j = s2v[j];
         const double ai = z1[i], aj = z1[j], di = z2[i], dj = z2[j];
-        const double xai = step ? dba[i] : 0.0, xaj = step ? dba[j] : 0.0;
-        const double xi = step ? db[i] : 0.0, xj = step ? db[j] : 0.0;
+        const double xai = step ? (double)dba[i] : 0.0, xaj = step ? (double)dba[j] : 0.0;
+        const double xi = step ? (double)db[i] : 0.0, xj = step ? (double)db[j] : 0.0;
         const double bei = beta[i], bej = beta[j], qi = Qb[i], qj = Qb[j], bbi = b[i], bbj = b[j];
         elem(i, s1i, s2i, ai, di, xai, xi, bei, qi, bbi);
         elem(j, s1j, s2j, aj, dj, xaj, xj, bej, qj, bbj);
     }
     if (i < n)
-        elem(i, s1v[i], s2v[i], z1[i], z2[i], step ? dba[i] : 0.0, step ? db[i] : 0.0, beta[i], Qb[i], b[i]);
+        elem(i, s1v[i], s2v[i], z1[i], z2[i], step ? (double)dba[i] : 0.0, step ? (double)db[i] : 0.0, beta[i], Qb[i],
+             b[i]);
     grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
 }
 
@@ -465,10 +468,11 @@ static __global__ void ipm_diag64_kernel(long long n, const double* __restrict__
 
 // beta += alpha db (the slacks and multipliers take their step in the next
 // residual pass)
-static __global__ void ipm_beta_step_kernel(long long n, double* __restrict__ beta, const double* __restrict__ db,
+template <typename TD>
+static __global__ void ipm_beta_step_kernel(long long n, double* __restrict__ beta, const TD* __restrict__ db,
                                             const double* __restrict__ alpha_p) {
     const double alpha = *alpha_p;
-    CSIPM_GRID_LOOP(i, n) beta[i] += alpha * db[i];
+    CSIPM_GRID_LOOP(i, n) beta[i] += alpha * (double)db[i];
 }
 
 // c = (s1 + s2)/2
