@@ -32,8 +32,23 @@ __device__ __forceinline__ C tw_apply(C v, const C* __restrict__ tw, int e) {
 }
 
 // ------------------------------------------------------------ strided pass
+// CTAs per SM the register allocation of a strided pass must allow, by
+// precision, CTA size (NT threads) and pass kind, as measured on B200 at
+// 256^3 and 320^3: more CTAs hide the gather/scatter load latency (the
+// scatter epilogue would otherwise take 88 FP32 / 148 FP64 registers and
+// leave 2 CTAs per SM), while the plain FP64 pass of 160-thread CTAs runs
+// fastest unconstrained.  (An explicit 1 lets the compiler use up to 255
+// registers, more than it picks with no bound at all.)
+template <typename T, int IN, int OUT, int NT> constexpr int fft2_min_ctas() {
+    constexpr bool scatter = OUT == OUT_SSCATTER || OUT == OUT_SCATTER;
+    if (sizeof(T) == 4) return scatter ? 3 : (NT <= 256 ? 4 : 3);
+    if (NT <= 128) return 4;
+    return scatter ? 3 : ((IN == IN_SGATHER || IN == IN_GATHER) ? 4 : 1);
+}
+
 template <typename T, int A, int B, bool INV, int IN, int OUT, typename TS, class Epi>
-__global__ void __launch_bounds__(fft2_tb<T>() * (A > B ? A : B))
+__global__ void __launch_bounds__(fft2_tb<T>() * (A > B ? A : B),
+                                  (fft2_min_ctas<T, IN, OUT, fft2_tb<T>() * (A > B ? A : B)>()))
 strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
     constexpr int TB = fft2_tb<T>();
