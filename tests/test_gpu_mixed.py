@@ -31,8 +31,10 @@ def _solve(torch, prob, precision, **kw):
 # (Stockham FP32 passes), 1D row passes
 @pytest.mark.parametrize("kind,dims", [("1d", (4096,)), ("1d", (24000,)), ("2d", (64, 64)), ("2d", (96, 128)), ("3d", (32, 32, 32)),
                                        ("3d", (32, 64, 24)), ("3d", (64, 64, 64))])
-@pytest.mark.parametrize("cg_rtol", [1e-8, 1e-5])
+@pytest.mark.parametrize("cg_rtol", [1e-8, 1e-5, 1e-2])
 def test_mixed_matches_fp64(cuda, kind, dims, cg_rtol):
+    """1e-2 runs the loose mode: FP32 Newton directions, corrector warm start
+    from the predictor's CG residual, FP64 barrier diagonals only on demand."""
     torch = cuda
     prob = _problem(kind, dims, seed=5)
     r64 = _solve(torch, prob, "fp64", tol=1e-10, ipm_cg_rtol=cg_rtol)
@@ -71,3 +73,19 @@ def test_mixed_uses_less_fp64_work(cuda):
     fp64_products = st["ipm_iter"] + 1 + st["ipm_iter"] + st["refinements"]
     assert st["matvecs"] >= st["cg_iter"]
     assert st["matvecs"] - st["cg_iter"] <= fp64_products
+
+
+def test_fp32_directions_through_fp64_refinement(cuda):
+    """Loose mode with one FP32 CG iteration per round: Newton solves that are
+    not done after it leave the FP32 iterate for FP64 refinement rounds and
+    come back to FP32 at the end; the solve still matches FP64."""
+    torch = cuda
+    prob = _problem("3d", (32, 64, 24), seed=3)
+    r64 = _solve(torch, prob, "fp64", tol=1e-10, ipm_cg_rtol=1e-2)
+    r32 = _solve(torch, prob, "mixed", tol=1e-10, ipm_cg_rtol=1e-2, cg_maxit=1, ir_max=10)
+    st = r32.stats
+    # FP64 products beyond the per-iteration residual A'A beta: refinement residuals
+    assert st["matvecs"] - st["cg_iter"] > st["ipm_iter"] + 1
+    b64, b32 = r64.beta.cpu().numpy(), r32.beta.cpu().numpy()
+    assert np.linalg.norm(b32 - b64) / np.linalg.norm(b64) <= 1e-6
+    assert abs(st["lasso_obj"] - r64.stats["lasso_obj"]) <= 1e-8 * abs(r64.stats["lasso_obj"])
