@@ -86,6 +86,9 @@ class Stats(ctypes.Structure):
         ("solve_ms", ctypes.c_double),
         ("launches", ctypes.c_longlong),
         ("fallbacks", ctypes.c_int),
+        ("resid_pass_ms", ctypes.c_double),
+        ("resid_pass_bytes", ctypes.c_double),
+        ("resid_pass_launches", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -631,6 +631,8 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     cudaMemsetAsync(h->slots, 0, sizeof(double) * SL_COUNT, h->stream);
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
+    cudaEventCreate(&h->ev_rp[0]);
+    cudaEventCreate(&h->ev_rp[1]);
     // A^T z0 (src/fft_model.jl:60-62) and ||z0||^2
     EpiStore<double> st_b{h->b};
     {
@@ -780,6 +782,16 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         h->launches += 1;   // pending s/z step + residual + barrier diagonals + predictor right-hand side
         const bool step = k > 0;
         h->diag64_stale = lazy64;
+        {
+            // algorithmic bytes: b, Qb, beta, s1, s2, z1, z2 read; rd, rhs written;
+            // with the pending step the two directions read and s, z written;
+            // the barrier diagonals written in FP64 and/or FP32
+            const double td = dir32 ? 4.0 : 8.0;
+            const double per = 56.0 + 16.0 + (step ? 2.0 * td + 32.0 : 0.0) + (lazy64 ? 0.0 : 16.0) + (mixed ? 8.0 : 0.0);
+            S.resid_pass_bytes += per * (double)n;
+            S.resid_pass_launches += 1;
+        }
+        cudaEventRecord(h->ev_rp[0], st);
         if (dir32)
             ew_launch(ipm_resdiag_kernel<float, float>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
                       step ? h->f_dba : nullptr, step ? h->f_db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
@@ -792,8 +804,13 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
                       mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
                       h->ws(h->slots + SL_RED));
         CK(cudaGetLastError());
+        cudaEventRecord(h->ev_rp[1], st);
         int r = read_slots(h, SL_RED, RR_N);
         if (r) return r;
+        {
+            float rp_ms = 0.f;   // the stream is synchronised: both events are complete
+            if (cudaEventElapsedTime(&rp_ms, h->ev_rp[0], h->ev_rp[1]) == cudaSuccess) S.resid_pass_ms += rp_ms;
+        }
         const double* R = h->hslots + SL_RED;
         mu = R[RR_SZ] / (2.0 * (double)n);
         const double usq = h->z0sq - 2.0 * R[RR_BB] + R[RR_BQB];

@@ -145,6 +145,7 @@ struct csipm_handle_s {
     long long launches = 0;
     double krylov_ms = 0.0, total_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_rp[2] = {nullptr, nullptr};   // around each residual pass
 
     cudaMemPool_t pool = nullptr;   // device_pool(device): every device buffer of the handle
     static constexpr size_t HSLOT_BYTES = sizeof(double) * 64;   // SL_COUNT slots
@@ -165,6 +166,8 @@ struct csipm_handle_s {
         if (hcgs) pinned_put(hcgs, HCGS_BYTES);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (auto& e : ev_rp)
+            if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 

@@ -59,8 +59,11 @@ mutable struct CsipmStats                # csipm_stats
     solve_ms::Cdouble
     launches::Clonglong
     fallbacks::Cint
+    resid_pass_ms::Cdouble
+    resid_pass_bytes::Cdouble
+    resid_pass_launches::Cint
 end
-CsipmStats() = CsipmStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+CsipmStats() = CsipmStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
 
 function csipm_check(st, h=C_NULL)
     st == 0 && return nothing

@@ -115,6 +115,12 @@ typedef struct {
     double solve_ms;           /* wall time of csipm_solve on the device stream */
     long long launches;        /* kernels the solve launched (including early-exit CG tails) */
     int fallbacks;             /* mixed precision: Newton solves finished in FP64 after an FP32 CG breakdown */
+    /* the residual pass (the solve's largest kernel: pending step, residual,
+     * barrier diagonals, predictor right-hand side), timed with CUDA events on
+     * the solve's stream around each launch */
+    double resid_pass_ms;      /* device time of all its launches */
+    double resid_pass_bytes;   /* their algorithmic bytes (vectors read + written) */
+    int resid_pass_launches;   /* its launches (IPM iterations + 1) */
 } csipm_stats;
 
 /* ---------------------------------------------------------------- lifecycle */
