@@ -137,6 +137,10 @@ void csipm_server_s::work(int slot) {
             dp.z0 = z0;
             csipm_options o = p.req.options;
             o.stream = st;
+            // a served handle lives for one solve: instantiating its CG-loop
+            // graphs on the slot threads costs more host time than the
+            // replays save (16 slots: 274 -> 352 solves/s without them)
+            o.cuda_graphs = 0;
             status = csipm_create(&dp, &o, &h);
         }
         if (status == CSIPM_OK) {

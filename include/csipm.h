@@ -333,7 +333,9 @@ typedef struct {
 
 typedef struct {
     csipm_problem problem;     /* as for csipm_create, but z0 is a HOST pointer (N reals) */
-    csipm_options options;     /* from csipm_default_options, then edited; `stream` is ignored */
+    csipm_options options;     /* from csipm_default_options, then edited; `stream` and
+                                  `cuda_graphs` are ignored (each request's handle lives for one
+                                  solve on its slot's stream; its CG loops run as plain launches) */
     double* beta_out;          /* HOST, N reals, written before the result is posted (may be NULL) */
     uint64_t tag;              /* the caller's id, returned with the result */
 } csipm_request;
