@@ -294,7 +294,7 @@ static void ensure_diag64(csipm_handle h) {
 }
 
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v, float* xf) {
+                const double* r0v, float* xf, bool ready) {
     const long long n = h->N;
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
@@ -306,7 +306,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
     // loose Newton tolerances take the warm-start residual from the FP32
     // product: its rounding (~1e-7 relative) is far below what they ask
     // a given warm-start residual serves round 0 with no product at all
-    const bool given = has_x0 && r0v != nullptr;
+    const bool given = has_x0 && (r0v != nullptr || ready);
     const bool fp32_warm = has_x0 && !given && rtol >= MIXED_FP32_WARM_RTOL;
     h->resid_kind = RESID_NONE;
     // with xf, round 0 iterates on xf itself (no correction vector, no FP64
@@ -354,9 +354,12 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
         }
         // FP32 PCG on K d = res: from d = 0 into f_x, or (in32) on xf from its start
         float* xi = in32 ? xf : h->f_x;
-        CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
+        const bool started = ready && round == 0 && in32;   // r, p and the CG scalars already written
+        if (!started) CK(cudaMemsetAsync(h->cgs, 0, sizeof(CgScalars), st));
         if (!in32) CK(cudaMemsetAsync(h->f_x, 0, sizeof(float) * n, st));
-        if (round == 0 && fp32_warm) {
+        if (started) {
+            // the FP32 CG starts from what the producing kernel wrote
+        } else if (round == 0 && fp32_warm) {
             // warm-start residual rhs - K x0 with the FP32 product (x0 rounded to FP32)
             const float* x0f = xf;
             if (!in32) {
@@ -374,7 +377,7 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
                                                              h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
         }
         CK(cudaGetLastError());
-        h->launches += 1;
+        if (!started) h->launches += 1;
         const int cap = std::min(maxit, MIXED_ROUND_MAXIT);
         auto iteration = [&](cudaStream_t s, int it) -> cudaError_t {
             EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
@@ -749,6 +752,8 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     // they are only asked to a relative accuracy >= 1e-4, far above FP32
     // rounding, and the IPM residual is recomputed in FP64 every iteration
     const bool dir32 = lazy64;
+    // relative tolerance of round 0 of a mixed Newton solve (schur_mixed)
+    const double cg_rin = std::max(o.ipm_cg_rtol, MIXED_INNER_RTOL);
     cudaEventRecord(h->ev0, st);
     // every beta-space vector of the solve is in solver order when h->sorder
     const double* bv = h->sorder ? h->bs : h->b;
@@ -785,9 +790,11 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         {
             // algorithmic bytes: b, Qb, beta, s1, s2, z1, z2 read; rd, rhs written;
             // with the pending step the two directions read and s, z written;
-            // the barrier diagonals written in FP64 and/or FP32
+            // the barrier diagonals written in FP64 and/or FP32; with FP32
+            // directions the predictor CG's r and p written
             const double td = dir32 ? 4.0 : 8.0;
-            const double per = 56.0 + 16.0 + (step ? 2.0 * td + 32.0 : 0.0) + (lazy64 ? 0.0 : 16.0) + (mixed ? 8.0 : 0.0);
+            const double per = 56.0 + 16.0 + (step ? 2.0 * td + 32.0 : 0.0) + (lazy64 ? 0.0 : 16.0) +
+                               (mixed ? 8.0 : 0.0) + (dir32 ? 8.0 : 0.0);
             S.resid_pass_bytes += per * (double)n;
             S.resid_pass_launches += 1;
         }
@@ -796,13 +803,13 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
             ew_launch(ipm_resdiag_kernel<float, float>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
                       step ? h->f_dba : nullptr, step ? h->f_db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
                       h->rd, (double*)nullptr, (double*)nullptr, h->f_Db, h->f_Minv, o.preconditioner, h->rhs,
-                      h->ws(h->slots + SL_RED));
+                      h->ws(h->slots + SL_RED), h->f_r, h->f_p, h->cgs, cg_rin);
         else
             ew_launch(ipm_resdiag_kernel<float, double>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1,
                       h->z2, step ? h->dba : nullptr, step ? h->db : nullptr, h->slots + SL_SIGMU,
                       h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
                       mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
-                      h->ws(h->slots + SL_RED));
+                      h->ws(h->slots + SL_RED), (float*)nullptr, (float*)nullptr, (CgScalars*)nullptr, 0.0);
         CK(cudaGetLastError());
         cudaEventRecord(h->ev_rp[1], st);
         int r = read_slots(h, SL_RED, RR_N);
@@ -835,7 +842,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         // ---- predictor (affine scaling): diagonals and right-hand side came with the residual
         int its = 0;
         int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its, nullptr,
-                                     dir32 ? h->f_dba : nullptr)
+                                     dir32 ? h->f_dba : nullptr, dir32)
                        : schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
@@ -858,22 +865,33 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         const int rk = (!mixed || o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL) ? h->resid_kind : RESID_NONE;
         const float* rp32 = rk == RESID_F32 ? h->f_r : nullptr;
         const double* rp64 = rk == RESID_CG64 ? h->cg_r : nullptr;
+        // FP32 directions with a known warm-start residual: this pass also
+        // starts the corrector's FP32 CG (r, p, scalars), replacing its init pass
+        const bool cstart = dir32 && rk != RESID_NONE;
+        float* cr = cstart ? h->f_r : nullptr;
+        float* cp = cstart ? h->f_p : nullptr;
+        const float* cm = o.preconditioner ? h->f_Minv : nullptr;
+        RedWorkspace cws = h->ws(h->slots + SL_DUMMY);
         if (dir32 && rp32)
             ew_launch(ipm_rhs_kernel<float, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp32, h->f_db);
+                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp32, h->f_db, cr, cp, cm, h->cgs, cws,
+                      cg_rin);
         else if (dir32)
             ew_launch(ipm_rhs_kernel<double, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp64, h->f_db);
+                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp64, h->f_db, cr, cp, cm, h->cgs, cws,
+                      cg_rin);
         else if (rp32)
             ew_launch(ipm_rhs_kernel<float, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp32, h->db);
+                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp32, h->db, (float*)nullptr,
+                      (float*)nullptr, (const float*)nullptr, (CgScalars*)nullptr, cws, 0.0);
         else
             ew_launch(ipm_rhs_kernel<double, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp64, h->db);
+                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp64, h->db, (float*)nullptr,
+                      (float*)nullptr, (const float*)nullptr, (CgScalars*)nullptr, cws, 0.0);
         CK(cudaGetLastError());
-        const double* r0v = rk != RESID_NONE ? h->rd : nullptr;
+        const double* r0v = rk != RESID_NONE && !cstart ? h->rd : nullptr;
         cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v,
-                                 dir32 ? h->f_db : nullptr)
+                                 dir32 ? h->f_db : nullptr, cstart)
                    : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }

@@ -385,13 +385,15 @@ enum { RESID_NONE = 0, RESID_CG64 = 1, RESID_F32 = 2 };   // none / FP64 in cg_r
 // Newton solves of the condensed system K x = rhs.  has_x0: x holds a start;
 // r0v (optional, with has_x0): rhs - K x0 is already known and no product
 // is spent on it.  xf (schur_mixed, optional): the start and the result are
-// held in FP32 there instead of x (x is then scratch).  On return
+// held in FP32 there instead of x (x is then scratch).  ready (with xf): the
+// kernel that produced the right-hand side (or the warm-start residual) also
+// wrote the FP32 CG start (f_r, f_p, h->cgs) for round 0.  On return
 // h->resid_kind says where the residual
 // rhs - K x of the result is held (RESID_*).
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
              const double* r0v = nullptr);
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v = nullptr, float* xf = nullptr);
+                const double* r0v = nullptr, float* xf = nullptr, bool ready = false);
 int ensure_kkt_buffers(csipm_handle h);
 int ensure_gondzio_buffers(csipm_handle h);
 

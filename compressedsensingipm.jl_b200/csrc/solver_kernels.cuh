@@ -36,6 +36,20 @@ struct CgScalars {
     int pad;
 };
 
+// CG scalars of a start whose r.(Minv r) = rz was reduced by the kernel that
+// wrote r and p (thresh = atol + rtol*sqrt(rz)); one thread.
+__device__ __forceinline__ void cg_start(CgScalars* sc, double rz, double atol, double rtol) {
+    sc->rz[0] = rz;
+    sc->rz[1] = 0.0;
+    sc->pq = 0.0;
+    sc->rz0 = rz;
+    sc->thresh = atol + rtol * sqrt(rz);
+    sc->iters = 0;
+    sc->breakdown = 0;
+    sc->done = (sqrt(rz) <= sc->thresh) ? 1 : 0;
+    if (!isfinite(rz)) { sc->done = 1; sc->breakdown = 1; }
+}
+
 // r = rhs - q (q = (Q + D) x0 computed by the operator), or r = rhs when x0 == 0;
 // z = Minv r ; p = z ; rz = r.z ; thresh = atol + rtol*sqrt(rz)
 template <typename TV>
@@ -142,7 +156,7 @@ static __global__ void add_f32_kernel(long long n, const float* __restrict__ d, 
 
 // ------------------------------------------------------------------ IPM state
 // Reductions of the residual kernel (component index):
-enum { RR_SZ = 0, RR_BB, RR_BQB, RR_L1, RR_GINF, RR_RDINF, RR_RCINF, RR_SUMC, RR_N };
+enum { RR_SZ = 0, RR_BB, RR_BQB, RR_L1, RR_GINF, RR_RDINF, RR_RCINF, RR_SUMC, RR_RZ, RR_N };
 constexpr unsigned RR_MAXMASK = (1u << RR_GINF) | (1u << RR_RDINF) | (1u << RR_RCINF);
 
 // beta = soft(b, lambda); reduce max|beta| and max|b|
@@ -241,12 +255,19 @@ __device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, dou
 // residual rhs - K dba = rhs - rhs_p + rp replaces rd (rd is not needed after
 // this pass; rhs still holds rhs_p on entry); with x0 the warm start
 // x0 = dba is written as well.
+//
+// With cr (FP32 corrector CG, rp given): the CG starts here instead of rd:
+// r = the warm-start residual, p = Minv r (cm: the rounded preconditioner,
+// null without one), r.(Minv r) reduced and the CG scalars set.  rp may be
+// the same vector as cr (read, then overwritten, by the same thread).
 template <typename TR, typename TD>
 static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
                                const TD* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
-                               const TR* __restrict__ rp, TD* __restrict__ x0) {
+                               const TR* rp, TD* __restrict__ x0, float* cr, float* __restrict__ cp,
+                               const float* __restrict__ cm, CgScalars* csc, RedWorkspace ws, double crtol) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
+    double acc[1] = {0.0};
     CSIPM_GRID_LOOP(i, n) {
         const ElemPre e = elem_pre(s1v[i], s2v[i], z1[i], z2[i]);
         double cor1 = 0.0, cor2 = 0.0;
@@ -260,10 +281,19 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
         const double fb = -rd[i] + h1 - h2;
         const double fc = -(lam - e.a - e.d) + h1 + h2;
         const double rn = fb - e.L2 * fc * e.iL1;
-        if (rp) rd[i] = rn - rhs[i] + (double)rp[i];
+        if (cr) {
+            const double r0 = rn - rhs[i] + (double)rp[i];
+            const double zv = cm ? (double)cm[i] * r0 : r0;
+            cr[i] = (float)r0;
+            cp[i] = (float)zv;
+            acc[0] += r0 * zv;
+        } else if (rp) {
+            rd[i] = rn - rhs[i] + (double)rp[i];
+        }
         rhs[i] = rn;
         if (x0) x0[i] = dba[i];
     }
+    if (cr && grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) cg_start(csc, ws.out[0], 0.0, crtol);
 }
 
 // Step statistics of a direction: min ratios (primal, dual) and the sums for mu_aff.
@@ -393,8 +423,9 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
                    const TD* __restrict__ db, const double* __restrict__ sigmu_p,
                    const double* __restrict__ alpha_p, double* __restrict__ rd, double* __restrict__ Db,
                    double* __restrict__ Minv, TV* __restrict__ Db_lo, TV* __restrict__ Minv_lo, int precond,
-                   double* __restrict__ rhs, RedWorkspace ws) {
-    double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+                   double* __restrict__ rhs, RedWorkspace ws, TV* __restrict__ cr, TV* __restrict__ cp,
+                   CgScalars* csc, double crtol) {
+    double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const bool step = db != nullptr;
     const double sigmu = step ? *sigmu_p : 0.0;
     const double alpha = step ? *alpha_p : 0.0;
@@ -431,7 +462,16 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
         const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
         if (Db) { Db[i] = dbv; Minv[i] = mi; }
         if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
-        rhs[i] = -r - a + d + L2 * lam * iL1;
+        const double v = -r - a + d + L2 * lam * iL1;
+        rhs[i] = v;
+        if (cr) {
+            // start of the predictor's FP32 CG (r = rhs, p = Minv r, from x = 0),
+            // with the rounded preconditioner the CG kernels read
+            const double zv = (double)(TV)mi * v;
+            cr[i] = (TV)v;
+            cp[i] = (TV)zv;
+            acc[RR_RZ] += v * zv;
+        }
     };
     // two elements per trip with all loads issued first (load latency)
     const long long G = (long long)gridDim.x * blockDim.x;
@@ -449,7 +489,7 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
     if (i < n)
         elem(i, s1v[i], s2v[i], z1[i], z2[i], step ? (double)dba[i] : 0.0, step ? (double)db[i] : 0.0, beta[i], Qb[i],
              b[i]);
-    grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u);
+    if (grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u) && csc && threadIdx.x == 0) cg_start(csc, ws.out[RR_RZ], 0.0, crtol);
 }
 
 // FP64 barrier diagonals alone (mixed precision at loose Newton tolerances
