@@ -204,17 +204,42 @@ static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ 
 // (three divisions; FP64 division is the expensive part of these kernels).
 struct ElemPre { double a, d, is1, is2, D1, D2, L2, iL1; };
 
+// One FP64 division per element: with p = s1 s2 and w = a s2 + d s1 (so
+// D1 + D2 = w/p), R = 1/(p w) gives 1/s1 = s2 w R, 1/s2 = s1 w R and
+// 1/(D1 + D2) = p p R.  Slacks and multipliers are strictly positive inside
+// the interior-point loop, so p w > 0; three IEEE divisions per element kept
+// the FP64 pipe of the step-statistics pass 41-47% busy.
 __device__ __forceinline__ ElemPre elem_pre(double s1, double s2, double a, double d) {
     ElemPre e;
     e.a = a;
     e.d = d;
-    e.is1 = 1.0 / s1;
-    e.is2 = 1.0 / s2;
+    const double p = s1 * s2;
+    const double w = fma(a, s2, d * s1);
+    const double R = 1.0 / (p * w);
+    const double u = w * R;   // 1/p
+    e.is1 = s2 * u;
+    e.is2 = s1 * u;
     e.D1 = a * e.is1;
     e.D2 = d * e.is2;
     e.L2 = e.D1 - e.D2;
-    e.iL1 = 1.0 / (e.D1 + e.D2);
+    e.iL1 = p * (p * R);
     return e;
+}
+
+// Barrier diagonal of the condensed Schur system and the fc weight of its
+// right-hand side, from one division: Db = 4 D1 D2/(D1 + D2) = 4 a d/w and
+// L2/L1 = (D1 - D2)/(D1 + D2) = (a s2 - d s1)/w with w = a s2 + d s1.  The
+// residual pass and the lazy FP64 diagonal kernel both use it, so their Db
+// agree bit for bit.
+struct ElemDiag { double db, l2l1; };
+
+__device__ __forceinline__ ElemDiag elem_diag(double s1, double s2, double a, double d) {
+    const double as2 = a * s2, ds1 = d * s1;
+    const double rw = 1.0 / (as2 + ds1);
+    ElemDiag g;
+    g.db = 4.0 * (a * d) * rw;
+    g.l2l1 = (as2 - ds1) * rw;
+    return g;
 }
 
 // Newton direction of one element given db, the centring target sigmu and the
@@ -456,13 +481,12 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
         acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
         acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
         acc[RR_SUMC] += ce;
-        const double D1 = a / s1, D2 = d / s2;
-        const double iL1 = 1.0 / (D1 + D2), L2 = D1 - D2;
-        const double dbv = 4.0 * D1 * D2 * iL1;
+        const ElemDiag g = elem_diag(s1, s2, a, d);
+        const double dbv = g.db;
         const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
         if (Db) { Db[i] = dbv; Minv[i] = mi; }
         if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
-        const double v = -r - a + d + L2 * lam * iL1;
+        const double v = -r - a + d + lam * g.l2l1;
         rhs[i] = v;
         if (cr) {
             // start of the predictor's FP32 CG (r = rhs, p = Minv r, from x = 0),
@@ -499,8 +523,7 @@ static __global__ void ipm_diag64_kernel(long long n, const double* __restrict__
                                          const double* __restrict__ z1, const double* __restrict__ z2,
                                          double* __restrict__ Db, double* __restrict__ Minv, int precond) {
     CSIPM_GRID_LOOP(i, n) {
-        const double D1 = z1[i] / s1[i], D2 = z2[i] / s2[i];
-        const double dbv = 4.0 * D1 * D2 * (1.0 / (D1 + D2));   // as in ipm_resdiag_kernel, bit for bit
+        const double dbv = elem_diag(s1[i], s2[i], z1[i], z2[i]).db;   // as in ipm_resdiag_kernel
         Db[i] = dbv;
         Minv[i] = precond ? 1.0 / (1.0 + dbv) : 1.0;
     }
