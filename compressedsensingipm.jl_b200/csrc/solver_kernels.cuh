@@ -226,18 +226,28 @@ __device__ __forceinline__ ElemPre elem_pre(double s1, double s2, double a, doub
     return e;
 }
 
-// Barrier diagonal of the condensed Schur system and the fc weight of its
-// right-hand side, from one division: Db = 4 D1 D2/(D1 + D2) = 4 a d/w and
-// L2/L1 = (D1 - D2)/(D1 + D2) = (a s2 - d s1)/w with w = a s2 + d s1.  The
-// residual pass and the lazy FP64 diagonal kernel both use it, so their Db
-// agree bit for bit.
-struct ElemDiag { double db, l2l1; };
+// Barrier diagonal of the condensed Schur system, its Jacobi preconditioner
+// and the fc weight of the right-hand side, from one division: with
+// w = a s2 + d s1 and q = 4 a d, Db = 4 D1 D2/(D1 + D2) = q/w,
+// Minv = 1/(1 + Db) = w/(w + q) and L2/L1 = (D1 - D2)/(D1 + D2) = (a s2 - d s1)/w,
+// all from R = 1/(w (w + q)).  The residual pass and the lazy FP64 diagonal
+// kernel both use it, so their Db and Minv agree bit for bit.
+struct ElemDiag { double db, mi, l2l1; };
 
-__device__ __forceinline__ ElemDiag elem_diag(double s1, double s2, double a, double d) {
+__device__ __forceinline__ ElemDiag elem_diag(double s1, double s2, double a, double d, bool precond) {
     const double as2 = a * s2, ds1 = d * s1;
-    const double rw = 1.0 / (as2 + ds1);
+    const double w = as2 + ds1, q = 4.0 * (a * d);
     ElemDiag g;
-    g.db = 4.0 * (a * d) * rw;
+    double rw;
+    if (precond) {
+        const double R = 1.0 / (w * (w + q));
+        rw = (w + q) * R;
+        g.mi = w * (w * R);
+    } else {
+        rw = 1.0 / w;
+        g.mi = 1.0;
+    }
+    g.db = q * rw;
     g.l2l1 = (as2 - ds1) * rw;
     return g;
 }
@@ -481,9 +491,8 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
         acc[RR_RDINF] = fmax(acc[RR_RDINF], fabs(r));
         acc[RR_RCINF] = fmax(acc[RR_RCINF], fabs(rc));
         acc[RR_SUMC] += ce;
-        const ElemDiag g = elem_diag(s1, s2, a, d);
-        const double dbv = g.db;
-        const double mi = precond ? 1.0 / (1.0 + dbv) : 1.0;
+        const ElemDiag g = elem_diag(s1, s2, a, d, precond);
+        const double dbv = g.db, mi = g.mi;
         if (Db) { Db[i] = dbv; Minv[i] = mi; }
         if (Db_lo) { Db_lo[i] = (TV)dbv; Minv_lo[i] = (TV)mi; }
         const double v = -r - a + d + lam * g.l2l1;
@@ -523,9 +532,9 @@ static __global__ void ipm_diag64_kernel(long long n, const double* __restrict__
                                          const double* __restrict__ z1, const double* __restrict__ z2,
                                          double* __restrict__ Db, double* __restrict__ Minv, int precond) {
     CSIPM_GRID_LOOP(i, n) {
-        const double dbv = elem_diag(s1[i], s2[i], z1[i], z2[i]).db;   // as in ipm_resdiag_kernel
-        Db[i] = dbv;
-        Minv[i] = precond ? 1.0 / (1.0 + dbv) : 1.0;
+        const ElemDiag g = elem_diag(s1[i], s2[i], z1[i], z2[i], precond);   // as in ipm_resdiag_kernel
+        Db[i] = g.db;
+        Minv[i] = g.mi;
     }
 }
 
