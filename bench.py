@@ -127,17 +127,79 @@ class Dist:
 
 # ----------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock, power and clock-event reasons sampled during the timed region.
+
+    NVML read queries every 5 ms from a thread (three headline solves last
+    about 0.16 s, shorter than the 200 ms period of `nvidia-smi -lms`); when
+    NVML cannot be opened, `nvidia-smi -lms 200`.  Both only read the GPU's
+    state."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
+    PERIOD_S = 0.005
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv") if os.path.isdir(
             os.path.join(ROOT, "gpurun_out")) else f"/tmp/csipm_clocks_{os.getpid()}.csv"
 
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(self.index).uuid)
+            return N, N.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _start_nvml(self):
+        import threading
+        N, h = self._nvml_handle()
+        reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or N.nvmlDeviceGetCurrentClocksThrottleReasons
+        self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+        self.samples = []
+        self.halt = threading.Event()
+
+        def run():
+            while not self.halt.is_set():
+                try:
+                    self.samples.append((float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)), int(reasons(h)),
+                                         N.nvmlDeviceGetPowerUsage(h) / 1000.0))
+                except Exception:
+                    pass
+                self.halt.wait(self.PERIOD_S)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+
+    def _stop_nvml(self):
+        self.halt.set()
+        self.thread.join(timeout=5)
+        if not self.samples:
+            return None
+        found = set()
+        with open(self.path, "w") as fh:
+            fh.write("# NVML every %g ms: sm_mhz, max_sm_mhz, power_w, event_reasons_hex\n" % (1e3 * self.PERIOD_S))
+            for sm, rs, pw in self.samples:
+                fh.write(f"{sm:.0f}, {self.max_mhz:.0f}, {pw:.1f}, {rs:#x}\n")
+                for nm, bit in self.REASON_BITS:
+                    if rs & bit:
+                        found.add(nm)
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(found), "samples": len(self.samples), "source": "nvml"}
+
     def start(self):
+        try:
+            self._start_nvml()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -147,6 +209,8 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            return self._stop_nvml()
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -171,7 +235,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi"}
 
 
 def measured_peaks():
