@@ -264,6 +264,19 @@ template <typename T, int A, int B> struct Row2Shape {
     static constexpr int PER_ROW = BASE + (((A - BASE) % 16) + 16) % 16;
     static constexpr int NTL = A > B ? A : B;
     static constexpr int ROWS = row2_rows(PER_ROW * (int)sizeof(cplx_t<T>));
+    // Minimum resident CTAs per SM in the launch bound.  FP32: 1, which lets
+    // ptxas give the (10, 16) pass 102 registers (5 CTAs per SM) where the
+    // bound without a CTA count gave 72 (7 CTAs per SM): 0.129 -> 0.115 ms
+    // at 320^3 on B200.  FP64 with A < 16: as many as shared memory holds
+    // (228 KB per SM, 1 KB reserved per CTA) at no more than 96 registers
+    // per thread (the (10, 16) pass: 5 CTAs per SM instead of 4 at 104
+    // registers; the FP64 solve measured within 0.3% either way).  A 64-
+    // register cap on the FP32 passes, and any cap on (16, 16), spilled.
+    static constexpr int SMEM = ROWS * PER_ROW * (int)sizeof(cplx_t<T>);
+    static constexpr int BY_SMEM = (228 * 1024) / (SMEM + 1024);
+    static constexpr int BY_REGS = 65536 / (ROWS * NTL * 96);
+    static constexpr int MINB_RAW = BY_SMEM < BY_REGS ? BY_SMEM : BY_REGS;
+    static constexpr int MINB = (sizeof(T) != 8 || A == 16 || MINB_RAW < 1) ? 1 : MINB_RAW;
 };
 
 // Two thread mappings share the CTA: the B-task phases (inverse step 1,
@@ -272,7 +285,7 @@ template <typename T, int A, int B> struct Row2Shape {
 // forward step 1: the B-point DFTs) give each row A consecutive threads, so
 // ROWS*A threads work in whole warps instead of A of every B lanes.
 template <typename T, int A, int B, int IN, int OUT, bool MASK>
-__global__ void __launch_bounds__(Row2Shape<T, A, B>::ROWS * Row2Shape<T, A, B>::NTL)
+__global__ void __launch_bounds__(Row2Shape<T, A, B>::ROWS * Row2Shape<T, A, B>::NTL, Row2Shape<T, A, B>::MINB)
 row2_kernel(PassArgs<T> a) {
     using C = cplx_t<T>;
     using Sh = Row2Shape<T, A, B>;
