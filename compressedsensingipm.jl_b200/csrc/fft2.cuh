@@ -268,13 +268,16 @@ template <typename T, int A, int B> struct Row2Shape {
     // ptxas give the (10, 16) pass 102 registers (5 CTAs per SM) where the
     // bound without a CTA count gave 72 (7 CTAs per SM): 0.129 -> 0.115 ms
     // at 320^3 on B200.  FP64 with A < 16: as many as shared memory holds
-    // (228 KB per SM, 1 KB reserved per CTA) at no more than 96 registers
-    // per thread (the (10, 16) pass: 5 CTAs per SM instead of 4 at 104
-    // registers; the FP64 solve measured within 0.3% either way).  A 64-
-    // register cap on the FP32 passes, and any cap on (16, 16), spilled.
+    // (228 KB per SM, 1 KB reserved per CTA) at up to 128 registers per
+    // thread: the (10, 16) pass keeps 4 CTAs per SM with 128 registers
+    // (104 with no CTA count); same-box A/B at 320^3: FP64 solve
+    // 0.0763 -> 0.0747 s, mixed 0.0529 -> 0.0524 s, where a 96-register cap
+    // (5 CTAs per SM) measured no gain and a count of 1 took 164 registers
+    // (3 CTAs per SM).  A 64-register cap on the FP32 passes, and any cap on
+    // (16, 16), spilled.
     static constexpr int SMEM = ROWS * PER_ROW * (int)sizeof(cplx_t<T>);
     static constexpr int BY_SMEM = (228 * 1024) / (SMEM + 1024);
-    static constexpr int BY_REGS = 65536 / (ROWS * NTL * 96);
+    static constexpr int BY_REGS = 65536 / (ROWS * NTL * 128);
     static constexpr int MINB_RAW = BY_SMEM < BY_REGS ? BY_SMEM : BY_REGS;
     static constexpr int MINB = (sizeof(T) != 8 || A == 16 || MINB_RAW < 1) ? 1 : MINB_RAW;
 };
