@@ -11,6 +11,13 @@ collective on the path); times are the max over ranks.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload 3d320|3d256|3d160|3d128|2d1024|1d16384] [--precision fp64|mixed]
 
+Beside the headline solve the line carries: the FP64 path at the same
+settings, the other measured configurations (1D 2^14, 2D 1024^2, 3D 256^3 in
+FP64) as legs, the serving stream, and one complete FP64 CPU-twin solve of
+the headline problem (the accuracy oracle and the CPU baseline).  The
+reference arm (--impl reference) runs that CPU solve alone, measured end to
+end.
+
 Prints ONE JSON line on rank 0.
 """
 from __future__ import annotations
@@ -22,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -39,9 +47,8 @@ WORKLOADS = {
     "1d16384": dict(kind="1d", dims=(16384,)),
 }
 METRIC = "s-to-solve 3D 320^3 (beta 1e-6 vs FP64)"
-ORACLE_TOL, ORACLE_CG_RTOL = 1e-12, 1e-10     # the FP64 accuracy oracle
-TIGHT_TOL, TIGHT_CG_RTOL = 1e-11, 1e-8        # FP64 with tight (reference-like) Newton solves
-IPM_VEC_PER_ITER = 4                           # CPU estimate: IPM elementwise work per iteration, in CG-update units
+ORACLE_TOL, ORACLE_CG_RTOL = 1e-12, 1e-10     # the FP64 device accuracy oracle
+LEGS = ("1d16384", "2d1024", "3d256")          # the other measured configurations (FP64)
 
 
 def parse():
@@ -57,9 +64,14 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10, help="IPM stop (relative duality gap / scaled KKT error)")
     ap.add_argument("--cg-rtol", type=float, default=1e-2,
                     help="relative tolerance of each Newton solve (inexact Newton; the library default is 1e-8)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU-twin solve of the headline problem (accuracy vs the CPU twin and the CPU "
+                         "baseline; about three minutes of host time at 320^3)")
+    ap.add_argument("--no-legs", action="store_true", help="skip the 1D / 2D / 3D-256 FP64 legs")
+    ap.add_argument("--clock-log", default=None,
+                    help="CSV file for the clock samples of the timed region (default: a temporary file)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--serve-requests", type=int, default=160,
+    ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests of the serving stream measured beside the headline solve (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
     ap.add_argument("--no-graphs", action="store_true",
@@ -141,12 +153,11 @@ class ClockSampler:
                    ("sw_power_cap", 0x4))
     PERIOD_S = 0.005
 
-    def __init__(self, index):
+    def __init__(self, index, path=None):
         self.index = index
         self.proc = None
         self.thread = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/csipm_clocks_{os.getpid()}.csv"
+        self.path = path or os.path.join(tempfile.gettempdir(), f"csipm_clocks_{os.getpid()}_gpu{index}.csv")
 
     def _nvml_handle(self):
         import pynvml as N
@@ -345,7 +356,7 @@ def run_ours(args):
         for _ in range(warmup):
             solve(model)
         stats = []
-        clocks = ClockSampler(local) if sample_clocks else None
+        clocks = ClockSampler(local, args.clock_log) if sample_clocks else None
         D.barrier()
         torch.cuda.synchronize()
         if clocks:
@@ -367,7 +378,7 @@ def run_ours(args):
 
     # ---- accuracy oracle: a tight FP64 device solve of the same problem
     # (untimed), and the FP64 path timed beside the headline solve at the
-    # same settings and with the reference's tight Newton solves
+    # same settings (the CPU-twin comparison comes at the end)
     def rel(a, b_):
         return float(torch.linalg.vector_norm(a - b_) / torch.linalg.vector_norm(b_))
 
@@ -385,15 +396,15 @@ def run_ours(args):
     accuracy["within_1e-6"] = accuracy["beta_rel_err"] <= 1e-6
     fp64 = None
     if args.precision == "mixed":
-        fp64 = {}
-        for name, kw64 in (("same_settings", kw), ("tight_newton", dict(tol=TIGHT_TOL, ipm_cg_rtol=TIGHT_CG_RTOL))):
-            nlp64 = csipm.FFTNLPModel(params, rdft=True, precision="fp64", **kw64)
-            ms64, last64, _, _ = timed(nlp64, args.steps, args.warmup, False)
-            fp64[name] = {"value": round(ms64 / 1000.0, 5), "tol": kw64["tol"],
-                          "newton_cg_rtol": kw64.get("ipm_cg_rtol", 1e-8), "ipm_iter": last64["ipm_iter"],
-                          "cg_iter": last64["cg_iter"], "matvecs": last64["matvecs"],
-                          "beta_rel_err": rel(sol[:N], beta_o), "speedup_mixed_vs_this": round(ms64 / ms, 3)}
-            nlp64.op_fft.close()
+        # the plain FP64 GPU path on the same problem at the same settings
+        nlp64 = csipm.FFTNLPModel(params, rdft=True, precision="fp64", **kw)
+        ms64, last64, _, _ = timed(nlp64, args.steps, args.warmup, False)
+        fp64 = {"value": round(ms64 / 1000.0, 5), "tol": args.tol, "newton_cg_rtol": args.cg_rtol,
+                "ipm_iter": last64["ipm_iter"], "cg_iter": last64["cg_iter"], "matvecs": last64["matvecs"],
+                "beta_rel_err": rel(sol[:N], beta_o), "speedup_mixed_vs_fp64": round(ms64 / ms, 3),
+                "what": "FP64 device solve of the same problem with the same options (tol, Newton rtol, forcing)"}
+        nlp64.op_fft.close()
+    beta_main_host = beta_main.cpu().numpy()
     del beta_main, beta_o
 
     # ---- end to end through the C ABI with host buffers (pinned), per step:
@@ -492,13 +503,98 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    nlp.op_fft.close()
+    del z0_dev, sol, sol_e2e, z0_e2e
+    torch.cuda.empty_cache()
+    if not args.no_legs:
+        out["legs"] = {name: run_leg(args, name, rank) for name in LEGS if name != args.workload}
     if args.serve_requests > 0:
         out["serving"] = run_serving(args, args.serve_requests, args.serve_slots, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(spec, z0_host, lam, last)
+        twin = cpu_twin_solve(spec.size, spec.keep, z0_host, lam, args.tol, args.cg_rtol)
+        out["cpu_baseline"] = twin["cpu_baseline"]
+        out["accuracy"]["vs_cpu_twin"] = twin_accuracy(twin, beta_main_host, last, z0_host, lam)
     D.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------- legs
+def run_leg(args, name, rank):
+    """One more measured configuration, FP64, at the headline's settings: the
+    solve timed with CUDA events (a few steps), its counts, the residual pass
+    and each pass of one CG product (roofline), and beta against the CPU twin
+    (1D, 2D) or a tight FP64 device solve (3D 256^3: the twin would take
+    minutes)."""
+    import torch
+    import csipm
+    from csipm import _native
+    wl = WORKLOADS[name]
+    spec, z0_host, lam, missing = build_problem(wl, seed=rank)
+    N = spec.N
+    L = csipm.lib()
+    z0_dev = torch.tensor(z0_host, device="cuda")
+    params = csipm.FFTParameters(len(spec.size), spec.size, z0_dev, lam, missing)
+    nlp = csipm.FFTNLPModel(params, rdft=True, precision="fp64", tol=args.tol, ipm_cg_rtol=args.cg_rtol)
+    sol = torch.empty(N, dtype=torch.float64, device="cuda")
+    st = _native.Stats()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def solve(model):
+        _native.check(L.csipm_solve(model.handle, ctypes.c_void_p(sol.data_ptr()), None, ctypes.byref(st)),
+                      model.handle)
+        return st.as_dict()
+
+    steps = max(1, min(args.steps, 5))
+    for _ in range(max(1, min(args.warmup, 3))):
+        solve(nlp)
+    stats = []
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        stats.append(solve(nlp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    last = stats[-1]
+    beta = sol.cpu().numpy()
+    peak, peak_kind = measured_peaks()
+    rp_ms = sum(x["resid_pass_ms"] for x in stats) / max(1, sum(x["resid_pass_launches"] for x in stats))
+    rp_bytes = sum(x["resid_pass_bytes"] for x in stats) / max(1, sum(x["resid_pass_launches"] for x in stats))
+    passes = profile_passes(L, nlp, N, reps=10)
+    mv_ms = sum(p["ms"] for p in passes)
+    mv_bytes = sum(p["bytes"] for p in passes)
+    leg = {
+        "workload": workload_config(args, wl)["workload"].replace(args.precision, "fp64"),
+        "value": round(ms / 1000.0, 6), "unit": "s", "steps": steps, "precision": "fp64",
+        "ipm_iter": last["ipm_iter"], "cg_iter": last["cg_iter"], "matvecs": last["matvecs"], "gap": last["gap"],
+        "roofline": {
+            "resid_pass": {"ms": round(rp_ms, 5), "GBps": round(rp_bytes / rp_ms / 1e6, 1),
+                           "frac": round(rp_bytes / rp_ms / 1e6 / peak, 4)},
+            "cg_product": {"ms": round(mv_ms, 5), "GBps": round(mv_bytes / mv_ms / 1e6, 1),
+                           "frac": round(mv_bytes / mv_ms / 1e6 / peak, 4),
+                           "passes": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in p.items()}
+                                      for p in passes]},
+            "peak": peak, "peak_kind": peak_kind,
+            "note": "small grids stream from L2 (126 MB): fractions of the HBM copy rate above 1 are L2 reads"},
+    }
+    if wl["kind"] in ("1d", "2d"):
+        twin = cpu_twin_solve(spec.size, spec.keep, z0_host, lam, args.tol, args.cg_rtol)
+        leg["accuracy"] = twin_accuracy(twin, beta, last, z0_host, lam)
+        leg["cpu_baseline"] = twin["cpu_baseline"]
+    else:
+        o = csipm.FFTNLPModel(params, rdft=True, precision="fp64", tol=ORACLE_TOL, ipm_cg_rtol=ORACLE_CG_RTOL)
+        solve(o)
+        bo = sol.cpu().numpy()
+        leg["accuracy"] = {"oracle": f"FP64 device solve, tol {ORACLE_TOL:g}, Newton rtol {ORACLE_CG_RTOL:g}",
+                           "beta_rel_err": float(np.linalg.norm(beta - bo) / np.linalg.norm(bo))}
+        o.op_fft.close()
+    nlp.op_fft.close()
+    del z0_dev, sol
+    torch.cuda.empty_cache()
+    return leg
 
 
 # ----------------------------------------------------------------------- serving
@@ -529,8 +625,10 @@ def serving_problems(n, seed0=1000):
 def run_serving(args, n_req, slots, rank):
     """Sequential plain solves of the stream (one request at a time through the
     C ABI from host buffers: create, solve, D2H, destroy) against the serving
-    loop: a closed run (all requests at t=0: capacity) and a Poisson run at an
-    offered rate of 5x the sequential rate (latency)."""
+    loop: closed runs (all requests at t=0: capacity) with each request's
+    iterations as plain launches and as one graph launch, then a Poisson run
+    of the faster mode at 80% of its closed capacity (latency under a load the
+    loop sustains)."""
     import torch
     import csipm
     from csipm import _native
@@ -560,14 +658,13 @@ def run_serving(args, n_req, slots, rank):
         return n_req / (time.perf_counter() - t0), int(sum(s != 0 for s in status))
 
     seq_rate, seq_failed = sequential(opts)
-    seq_default_rate, seq_default_failed = sequential(dict(tol=1e-8, autotune=False))
 
-    def serve(rate):
+    def serve(rate, graphs):
         rng = np.random.default_rng(7)
         gaps = rng.exponential(1.0 / rate, size=n_req) if rate else np.zeros(n_req)
         arrivals = np.cumsum(gaps) - gaps[0]
         res = []
-        with Server(slots=slots) as srv:
+        with Server(slots=slots, cuda_graphs=graphs) as srv:
             t_start = time.perf_counter()
             for k, r in enumerate(reqs):
                 while True:
@@ -590,8 +687,12 @@ def run_serving(args, n_req, slots, rank):
         for k, r in enumerate(reqs[:slots]):
             srv.submit(r["size"], r["z0"], r["lam"], r["missing"], tag=k, precision=r["precision"], **opts)
         srv.drain()
-    closed = serve(0.0)
-    poisson = serve(5.0 * seq_rate)
+    closed_plain = serve(0.0, False)
+    closed_graphs = serve(0.0, True)
+    graphs = closed_graphs["solves_per_s"] > closed_plain["solves_per_s"]
+    closed = closed_graphs if graphs else closed_plain
+    offered = 0.8 * closed["solves_per_s"]
+    poisson = serve(offered, graphs)
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("1d", "2d", "3d")}
     return {
         "requests": n_req, "slots": slots, "mix": kinds,
@@ -600,88 +701,95 @@ def run_serving(args, n_req, slots, rank):
         "newton_cg_rtol": SERVE_CG_RTOL,
         "sequential_plain": {"solves_per_s": round(seq_rate, 2), "failed": seq_failed,
                              "what": "one request at a time through create/solve/D2H/destroy, same options"},
-        "sequential_default_options": {"solves_per_s": round(seq_default_rate, 2), "failed": seq_default_failed,
-                                       "what": "one at a time with the library defaults (Newton CG rtol 1e-8)"},
-        "batched_closed": closed,
-        "batched_poisson": dict(poisson, offered_per_s=round(5.0 * seq_rate, 2)),
+        "batched_closed": dict(closed, cuda_graphs=graphs),
+        "batched_closed_plain_launches": closed_plain,
+        "batched_closed_graph_launches": closed_graphs,
+        "batched_poisson": dict(poisson, offered_per_s=round(offered, 2), cuda_graphs=graphs),
         "speedup_vs_sequential": round(closed["solves_per_s"] / seq_rate, 2),
-        "speedup_vs_sequential_default_options": round(closed["solves_per_s"] / seq_default_rate, 2),
     }
 
 
-# ----------------------------------------------------------------------- CPU baseline (oracle)
-def _cpu_sample(size, keep, z0, lam, reps):
-    """Times the oracle's FP64 A^T A and one Schur-CG vector update on the full grid."""
+# ----------------------------------------------------------------------- CPU twin (oracle)
+def cpu_twin_solve(size, keep, z0, lam, tol, cg_rtol, on_iter=None):
+    """One complete FP64 CPU solve of the problem with the oracle's twin of the
+    device method (oracle_ipm.ipm: numpy elementwise work, scipy.fft pocketfft
+    products with one worker per host core), timed end to end from A^T z0 to
+    beta.  Returns beta, the twin's info and the cpu_baseline object."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
+    import oracle_ipm as OI
     cores = os.cpu_count() or 1
     op = O.Operator(size, keep, True, workers=cores)
+    op.AtA(np.zeros(int(np.prod(size))))   # pocketfft plan set-up, untimed
+    op.n_matvec, op.t_matvec = 0, 0.0
+    t0 = time.perf_counter()
     b = op.At(z0)
-    x = np.random.default_rng(0).standard_normal(b.size)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        q = op.AtA(x)
-    t_mv = (time.perf_counter() - t0) / reps
-    Db = np.abs(x)
-    Minv = 1.0 / (1.0 + Db)
-    r = b.copy()
-    p = Minv * r
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        q = q + Db * p
-        pq = p @ q
-        x += (1.0 / pq) * p
-        r -= (1.0 / pq) * q
-        rz = r @ (Minv * r)
-        p = Minv * r + rz * p
-    t_vec = (time.perf_counter() - t0) / reps
-    return t_mv, t_vec, cores
+    beta, _, info = OI.ipm(op, b, lam, float(z0 @ z0), tol=tol, cg_rtol=cg_rtol, on_iter=on_iter)
+    total = time.perf_counter() - t0
+    t_cg_vec = info["t_newton"] - info["t_newton_products"]
+    grid = "x".join(map(str, size))
+    return {
+        "beta": beta, "info": info, "op": op, "seconds": total,
+        "cpu_baseline": {
+            "value": round(total, 3), "unit": "s", "cores": cores, "kind": "port",
+            "sample": (f"one complete FP64 CPU solve of the same {grid} problem, measured end to end (not "
+                       f"extrapolated): the oracle's twin of the device method (numpy elementwise work on one "
+                       f"core, scipy.fft pocketfft products with workers={cores}) at the same tol {tol:g}, "
+                       f"Newton rtol {cg_rtol:g} and forcing term; {info['ipm_iter']} IPM iterations, "
+                       f"{info['cg_iter']} CG iterations, {op.n_matvec} products ({op.t_matvec:.1f} s), CG vector "
+                       f"work {t_cg_vec:.1f} s, IPM elementwise work {total - op.t_matvec - t_cg_vec:.1f} s"),
+            "status": info["status"],
+        },
+    }
 
 
-def cpu_baseline(spec, z0, lam, stats):
-    t_mv, t_vec, cores = _cpu_sample(spec.size, spec.keep, z0, lam, reps=2)
-    est = stats["matvecs"] * t_mv + (stats["cg_iter"] + IPM_VEC_PER_ITER * stats["ipm_iter"]) * t_vec
-    return {"value": round(est, 2), "unit": "s", "cores": cores, "kind": "port",
-            "sample": (f"oracle FP64 (numpy + scipy.fft pocketfft, workers={cores}) on the full grid: 2 A^T A "
-                       f"products ({t_mv:.2f} s each) and 2 CG vector updates ({t_vec:.2f} s each), scaled by "
-                       f"this solve's {stats['matvecs']} products, {stats['cg_iter']} CG iterations and "
-                       f"{IPM_VEC_PER_ITER} vector-update equivalents per IPM iteration ({stats['ipm_iter']})")}
+def twin_accuracy(twin, beta_gpu, stats, z0, lam):
+    """beta, the LASSO objective and the iteration count of a device solve
+    against the CPU twin of the same problem."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ipm as OI
+    bc = twin["beta"]
+    Fg = OI.lasso_value(twin["op"], beta_gpu, z0, lam)
+    Fc = OI.lasso_value(twin["op"], bc, z0, lam)
+    rel = float(np.linalg.norm(beta_gpu - bc) / np.linalg.norm(bc))
+    return {"oracle": "FP64 CPU twin solve of the same problem (oracle_ipm.ipm), same settings",
+            "beta_rel_err": rel, "lasso_obj_rel_err": abs(Fg - Fc) / abs(Fc),
+            "ipm_iter": stats["ipm_iter"], "ipm_iter_twin": twin["info"]["ipm_iter"],
+            "within_1e-6": rel <= 1e-6}
 
 
 def run_reference(args):
+    """The reference arm: the reference's path on the host cores.  Julia,
+    MadNLP and FFTW are not installed, so it is the oracle's FP64 twin of the
+    path (same maps, operator, condensed KKT and IPM algorithm) on the same
+    workload and settings as the GPU arm.  The warm-up builds the problem and
+    sets up the FFT plans; then ONE complete solve is measured end to end,
+    one IPM iteration per step (a solve that needs more iterations than
+    --steps runs them all; each iteration's seconds are listed), so `value`
+    is a measured s-to-solve, not an extrapolation."""
     world, rank, local = dist_setup(args)
     if rank != 0:
         return
     wl = WORKLOADS[args.workload]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    import oracle_ipm as OI
     import csipm.problems as P
     cores = os.cpu_count() or 1
-    # iteration counts from a full CPU solve of a reduced instance of the same generator
-    small = tuple(max(2, (d // 5) // 2 * 2) for d in wl["dims"]) if wl["kind"] == "3d" else wl["dims"]
-    sspec = P.make_spec(wl["kind"], dims=small, seed=0)
-    op0 = O.Operator(sspec.size, None, True, workers=cores)
-    sprob = P.finalize(sspec, op0.A, op0.At)
-    sop = O.Operator(sspec.size, sspec.keep, True, workers=cores)
-    sb = sop.At(sprob.z0)
-    sop.n_matvec = 0
-    # the reference's Newton solves are tight (Krylov atol 1e-12, rtol 0): CG rtol 1e-8 here
-    _, _, info = OI.ipm(sop, sb, sprob.lam, float(sprob.z0 @ sprob.z0), tol=args.tol, cg_rtol=1e-8)
-    counts = {"matvecs": sop.n_matvec, "cg_iter": info["cg_iter"], "ipm_iter": info["ipm_iter"]}
     spec = P.make_spec(wl["kind"], dims=wl["dims"], seed=0)
     opf = O.Operator(spec.size, None, True, workers=cores)
     prob = P.finalize(spec, opf.A, opf.At)
-    vals = []
-    for s in range(args.warmup + args.steps):
-        t_mv, t_vec, _ = _cpu_sample(spec.size, spec.keep, prob.z0, prob.lam, reps=1)
-        if s >= args.warmup:
-            vals.append(counts["matvecs"] * t_mv + (counts["cg_iter"] + IPM_VEC_PER_ITER * counts["ipm_iter"]) * t_vec)
-    v = float(np.mean(vals))
-    sample = (f"CPU FP64 port of the path (numpy + scipy.fft pocketfft, workers={cores}); per step one A^T A "
-              f"product and one CG vector update timed on the full {'x'.join(map(str, wl['dims']))} grid, scaled by "
-              f"the iteration counts of a full CPU solve of the same generator at {'x'.join(map(str, small))} "
-              f"({counts['ipm_iter']} IPM iterations, {counts['cg_iter']} CG iterations, {counts['matvecs']} products)")
+    del opf
+    marks = []
+    t_start = [None]
+
+    def on_iter(k, gap):
+        marks.append(time.perf_counter())
+
+    t_start[0] = time.perf_counter()
+    twin = cpu_twin_solve(spec.size, spec.keep, prob.z0, prob.lam, args.tol, args.cg_rtol, on_iter=on_iter)
+    v = twin["seconds"]
+    # seconds of each step: A'z0 + warm start + the first stop test, then one IPM iteration each
+    iters = [round(b_ - a_, 3) for a_, b_ in zip([t_start[0]] + marks[:-1], marks)]
     out = {
         "impl": "reference",
         "metric": METRIC if args.workload == "3d320" else f"s-to-solve {args.workload}",
@@ -690,14 +798,19 @@ def run_reference(args):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(v * 1000, 1),
+        "ms_per_step": round(1000.0 * v / max(1, len(iters)), 1),
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
         "config": workload_config(args, wl),
-        "cpu_baseline": {"value": round(v, 3), "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+        "measured": {"what": "one complete CPU solve, one IPM iteration per step (step 1 also holds A^T z0 and "
+                             "the warm start); value = the whole solve",
+                     "solve_steps": len(iters), "step_s": iters, "ipm_iter": twin["info"]["ipm_iter"],
+                     "cg_iter": twin["info"]["cg_iter"], "products": twin["op"].n_matvec,
+                     "status": twin["info"]["status"]},
+        "cpu_baseline": twin["cpu_baseline"],
         "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

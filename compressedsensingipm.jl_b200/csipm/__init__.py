@@ -138,7 +138,7 @@ class FFTParameters:
 
 def _options(rdft=True, precision="fp64", preconditioner=True, tol=1e-8, max_iter=2000, cg_atol=1e-12,
              cg_rtol=0.0, cg_maxit=0, ipm_cg_rtol=1e-8, ir_max=3, verbose=False, stream=None, layout="solver",
-             cuda_graphs=True, autotune=True):
+             cuda_graphs=True, autotune=True, ipm_cg_forcing=100.0):
     o = _native.Options()
     check(lib().csipm_default_options(ctypes.byref(o)))
     o.rdft = int(bool(rdft))
@@ -156,6 +156,7 @@ def _options(rdft=True, precision="fp64", preconditioner=True, tol=1e-8, max_ite
     o.layout = {"solver": 0, "reference": 1}[layout] if isinstance(layout, str) else int(layout)
     o.cuda_graphs = int(bool(cuda_graphs))
     o.autotune = int(bool(autotune))
+    o.ipm_cg_forcing = float(ipm_cg_forcing)
     return o
 
 

@@ -68,6 +68,7 @@ class Options(ctypes.Structure):
         ("layout", ctypes.c_int),
         ("cuda_graphs", ctypes.c_int),
         ("autotune", ctypes.c_int),
+        ("ipm_cg_forcing", ctypes.c_double),
     ]
 
 
@@ -89,6 +90,7 @@ class Stats(ctypes.Structure):
         ("resid_pass_ms", ctypes.c_double),
         ("resid_pass_bytes", ctypes.c_double),
         ("resid_pass_launches", ctypes.c_int),
+        ("graph_iters", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -104,7 +106,8 @@ class AdmmStats(ctypes.Structure):
 
 
 class ServerOptions(ctypes.Structure):
-    _fields_ = [("slots", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("device", ctypes.c_int)]
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("device", ctypes.c_int),
+                ("cuda_graphs", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):
@@ -113,7 +116,7 @@ class Request(ctypes.Structure):
 
 class Result(ctypes.Structure):
     _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int), ("stats", Stats), ("queue_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_size_t)]
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_size_t), ("message", ctypes.c_char * 160)]
 
 
 

@@ -42,14 +42,16 @@ class ServeResult:
     latency_ms: float
     footprint: int
     beta: np.ndarray = field(repr=False, default=None)
+    message: str = ""               # the failure's message when status != 0
 
 
 class Server:
     """csipm_server: `slots` concurrent solves within `hbm_budget` device bytes
-    (0: 80% of the free memory)."""
+    (0: 80% of the free memory); cuda_graphs: each request's iterations as one
+    graph launch."""
 
-    def __init__(self, slots=8, hbm_budget=0, device=-1):
-        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device))
+    def __init__(self, slots=8, hbm_budget=0, device=-1, cuda_graphs=False):
+        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device), int(bool(cuda_graphs)))
         h = ctypes.c_void_p()
         check(lib().csipm_server_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
@@ -98,7 +100,8 @@ class Server:
             r = buf[k]
             z0, miss, beta, _ = self._live.pop(int(r.tag))
             out.append(ServeResult(int(r.tag), int(r.status), r.stats.as_dict(), float(r.queue_ms),
-                                   float(r.latency_ms), int(r.footprint), beta))
+                                   float(r.latency_ms), int(r.footprint), beta,
+                                   r.message.decode(errors="replace")))
         return out
 
     def drain(self) -> list[ServeResult]:

@@ -220,7 +220,7 @@ int ew_grid(const void* kernel, long long n) {
 }
 
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-             const double* r0v) {
+             const double* r0v, const double* rtol_dev) {
     const long long n = h->N;
     cudaStream_t st = h->stream;
     const double* Minv = h->opt.preconditioner ? h->Minv : nullptr;
@@ -240,7 +240,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
         CK(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     }
     ew_launch(cg_init_kernel<double>, n, st, n, rhs, h->cg_q, has_x0 ? 1 : 0, Minv, h->cg_r, h->cg_p,
-                                                    h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rtol);
+                                                    h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, DevScalar(rtol, rtol_dev));
     CK(cudaGetLastError());
     h->launches += 1;
     auto iteration = [&](cudaStream_t s, int it) -> cudaError_t {
@@ -280,6 +280,9 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
 // FP32 breakdown (p.q <= 0 from rounding on a nearly singular direction)
 // keeps the partial correction and finishes the solve with FP64 PCG.
 constexpr double MIXED_INNER_RTOL = 1e-6;
+// floor of csipm_solve's forcing term: no Newton solve is asked for more than
+// FP32 products reach, so FP64 and mixed precision take the same iterates
+constexpr double CG_FORCING_FLOOR = 1e-6;
 constexpr double MIXED_FP32_WARM_RTOL = 1e-4;
 constexpr int MIXED_ROUND_MAXIT = 100;
 
@@ -294,7 +297,7 @@ static void ensure_diag64(csipm_handle h) {
 }
 
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v, float* xf, bool ready) {
+                const double* r0v, float* xf, bool ready, const double* rin_dev) {
     const long long n = h->N;
     cudaStream_t st = h->stream;
     const bool pc = h->opt.preconditioner != 0;
@@ -371,10 +374,12 @@ int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, doubl
             h->matvecs++;
             h->launches += ppp + 1;
             ew_launch(cg_init_kernel<float>, n, st, n, rhs, h->f_q, 1, Minv32, h->f_r, h->f_p,
-                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
+                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0,
+                                                             DevScalar(rin, round == 0 ? rin_dev : nullptr));
         } else {
             ew_launch(cg_init_kernel<float>, n, st, n, res, (const float*)nullptr, 0, Minv32, h->f_r, h->f_p,
-                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, rin);
+                                                             h->ws(h->slots + SL_DUMMY), h->cgs, 0.0,
+                                                             DevScalar(rin, round == 0 ? rin_dev : nullptr));
         }
         CK(cudaGetLastError());
         if (!started) h->launches += 1;
@@ -515,6 +520,316 @@ int profile_impl(csipm_handle h, FftOperator<T>& op, const T* x, T* D, T* q, int
     return CSIPM_OK;
 }
 
+
+// ------------------------------------------------------------------ IPM iteration pieces
+// What csipm_solve's options make of an iteration.
+struct IpmMode {
+    bool mixed;
+    bool lazy64;      // mixed precision: FP64 barrier diagonals only when a solve asks for them
+    bool dir32;       // mixed precision: Newton directions kept in FP32 (f_dba, f_db)
+    bool graphable;   // every iteration fits one graph replay (no host decision inside)
+};
+
+IpmMode ipm_mode(csipm_handle h) {
+    const csipm_options& o = h->opt;
+    IpmMode m{};
+    m.mixed = o.precision == CSIPM_MIXED;
+    // mixed precision with a Newton tolerance the FP32 warm start serves:
+    // the FP64 barrier diagonals are only computed when a solve needs them,
+    // and the Newton directions stay in FP32 (they are only asked to a
+    // relative accuracy >= 1e-4, far above FP32 rounding, and the IPM
+    // residual is recomputed in FP64 every iteration)
+    m.lazy64 = m.mixed && o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL;
+    m.dir32 = m.lazy64;
+    // graph replays: FP64, or mixed with FP32 directions (whose Newton solves
+    // are one FP32 CG each: the forcing term's floor is the FP32 round's);
+    // refinement rounds and fallbacks decide on the host
+    m.graphable = o.cuda_graphs && !o.verbose && (!m.mixed || m.dir32);
+    return m;
+}
+
+// The residual pass: the pending step on s and z (step), the dual residual,
+// the reductions of the stop test, the barrier diagonals and the predictor's
+// right-hand side; with FP32 directions also the start of the predictor's
+// FP32 CG at the tolerance *crtol.
+cudaError_t launch_resid_pass(csipm_handle h, cudaStream_t st, const IpmMode& md, bool step, const double* crtol) {
+    const long long n = h->N;
+    const double lam = h->lambda;
+    const bool pc = h->opt.preconditioner != 0;
+    const double* bv = h->sorder ? h->bs : h->b;
+    if (md.dir32)
+        ew_launch(ipm_resdiag_kernel<float, float>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
+                  step ? h->f_dba : nullptr, step ? h->f_db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
+                  h->rd, (double*)nullptr, (double*)nullptr, h->f_Db, h->f_Minv, pc ? 1 : 0, h->rhs,
+                  h->ws(h->slots + SL_RED), h->f_r, h->f_p, h->cgs, DevScalar(0.0, crtol));
+    else
+        ew_launch(ipm_resdiag_kernel<float, double>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
+                  step ? h->dba : nullptr, step ? h->db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
+                  h->rd, md.lazy64 ? nullptr : h->Db, md.lazy64 ? nullptr : h->Minv,
+                  md.mixed ? h->f_Db : nullptr, md.mixed ? h->f_Minv : nullptr, pc ? 1 : 0, h->rhs,
+                  h->ws(h->slots + SL_RED), (float*)nullptr, (float*)nullptr, (CgScalars*)nullptr, DevScalar());
+    return cudaGetLastError();
+}
+
+// The corrector's right-hand side after the predictor's step statistics and
+// centring target; rk says where the predictor left its residual (RESID_*),
+// from which the corrector's warm-start residual is formed with no product.
+// FP32 directions with a known residual: this pass also starts the
+// corrector's FP32 CG (r, p, scalars) at the tolerance *crtol.
+cudaError_t launch_corrector_rhs(csipm_handle h, cudaStream_t st, const IpmMode& md, int rk, const double* crtol) {
+    const long long n = h->N;
+    const double lam = h->lambda;
+    const float* rp32 = rk == RESID_F32 ? h->f_r : nullptr;
+    const double* rp64 = rk == RESID_CG64 ? h->cg_r : nullptr;
+    const double* sigmu_d = h->slots + SL_SIGMU;
+    const bool cstart = md.dir32 && rk != RESID_NONE;
+    float* cr = cstart ? h->f_r : nullptr;
+    float* cp = cstart ? h->f_p : nullptr;
+    const float* cm = h->opt.preconditioner ? h->f_Minv : nullptr;
+    RedWorkspace cws = h->ws(h->slots + SL_DUMMY);
+    if (md.dir32 && rp32)
+        ew_launch(ipm_rhs_kernel<float, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                  (const float*)h->f_dba, sigmu_d, h->rhs, rp32, h->f_db, cr, cp, cm, h->cgs, cws,
+                  DevScalar(0.0, crtol));
+    else if (md.dir32)
+        ew_launch(ipm_rhs_kernel<double, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                  (const float*)h->f_dba, sigmu_d, h->rhs, rp64, h->f_db, cr, cp, cm, h->cgs, cws,
+                  DevScalar(0.0, crtol));
+    else if (rp32)
+        ew_launch(ipm_rhs_kernel<float, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                  (const double*)h->dba, sigmu_d, h->rhs, rp32, h->db, (float*)nullptr, (float*)nullptr,
+                  (const float*)nullptr, (CgScalars*)nullptr, cws, DevScalar());
+    else
+        ew_launch(ipm_rhs_kernel<double, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
+                  (const double*)h->dba, sigmu_d, h->rhs, rp64, h->db, (float*)nullptr, (float*)nullptr,
+                  (const float*)nullptr, (CgScalars*)nullptr, cws, DevScalar());
+    return cudaGetLastError();
+}
+
+// After the corrector: its step statistics, the step length and the beta
+// step (s and z take the same step inside the next residual pass).
+cudaError_t launch_step(csipm_handle h, cudaStream_t st, const IpmMode& md) {
+    const long long n = h->N;
+    const double lam = h->lambda;
+    const double* sigmu_d = h->slots + SL_SIGMU;
+    double* alpha_d = h->slots + SL_ALPHA;
+    if (md.dir32)
+        ew_launch(ipm_stepstats_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, (const float*)h->f_dba,
+                  sigmu_d, (const float*)h->f_db, h->ws(h->slots + SL_SS));
+    else
+        ew_launch(ipm_stepstats_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, (const double*)h->dba,
+                  sigmu_d, (const double*)h->db, h->ws(h->slots + SL_SS));
+    ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, h->ctl, alpha_d);
+    if (md.dir32)
+        ew_launch(ipm_beta_step_kernel<float>, n, st, n, h->beta, (const float*)h->f_db, (const double*)alpha_d);
+    else
+        ew_launch(ipm_beta_step_kernel<double>, n, st, n, h->beta, (const double*)h->db, (const double*)alpha_d);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ IPM iteration graph
+// Adds a conditional node to the graph stream s is capturing: a handle on
+// that graph, set_fn(s, hnd) captured before the node (the kernel that sets
+// the handle each time the node is reached), the node itself, then
+// body_fn(s2, hnd) captured into the node's body on stream s2.  Afterwards s
+// depends on the node.
+template <class SetFn, class BodyFn>
+bool capture_conditional(cudaStream_t s, cudaStream_t s2, cudaGraphConditionalNodeType type, SetFn&& set_fn,
+                         BodyFn&& body_fn) {
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, &deps, &nd) != cudaSuccess || cst != cudaStreamCaptureStatusActive)
+        return false;
+    cudaGraphConditionalHandle hnd = 0;
+    if (cudaGraphConditionalHandleCreate(&hnd, g, 0, 0) != cudaSuccess) return false;
+    if (!set_fn(s, hnd)) return false;
+    if (cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, &deps, &nd) != cudaSuccess) return false;
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = hnd;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, g, deps, nd, &p) != cudaSuccess) return false;
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return false;
+    if (cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return false;
+    const bool ok = body_fn(s2, hnd);
+    cudaGraph_t out = nullptr;
+    const bool ended = cudaStreamEndCapture(s2, &out) == cudaSuccess;
+    return ok && ended;
+}
+
+// The graph of whole interior-point iterations (FP64, or mixed precision
+// with FP32 directions): a conditional WHILE node whose body is the rest of
+// one iteration after its stop test — predictor CG (a nested WHILE node),
+// then, if it converged, the step statistics, centring target, corrector
+// right-hand side and corrector CG, then, if that converged, the step, the
+// next A'A product, the next residual pass and its stop test, which keeps
+// the outer loop going while the method runs.  A CG breakdown, or a loop cap
+// below the solve's, ends the replay with the iteration handed back to the
+// host (IPM_ABORT).  Captured once per handle.
+bool build_ipm_graph(csipm_handle h, const IpmMode& md) {
+    const long long n = h->N;
+    const int maxit = h->opt.cg_maxit;
+    const bool pc = h->opt.preconditioner != 0;
+    const double* Minv = pc ? h->Minv : nullptr;
+    const float* Minv32 = pc ? h->f_Minv : nullptr;
+    const int cap = md.dir32 ? std::min(maxit, MIXED_ROUND_MAXIT) : std::min(maxit, CG_WHILE_CAP);
+    const int cap_is_limit = cap >= maxit ? 1 : 0;
+    const double* rt_dev = &h->ctl->rt;
+    int kernels = 0;
+    cudaStream_t ss[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (auto& x : ss)
+        if (cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) != cudaSuccess) x = nullptr;
+    cudaGraph_t graph = nullptr;
+    bool ok = ss[4] != nullptr && cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle loop = 0;
+    cudaGraphNodeParams lp = {};
+    cudaGraphNode_t lnode = nullptr;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        lp.type = cudaGraphNodeTypeConditional;
+        lp.conditional.handle = loop;
+        lp.conditional.type = cudaGraphCondTypeWhile;
+        lp.conditional.size = 1;
+        ok = cudaGraphAddNode(&lnode, graph, nullptr, 0, &lp) == cudaSuccess;
+    }
+    // one CG loop over the iterate x (FP64) or xf (FP32)
+    auto cg_loop = [&](cudaStream_t s, cudaStream_t sb, double* x, float* xf) -> bool {
+        auto arm = [&](cudaStream_t q, cudaGraphConditionalHandle hc) {
+            cg_arm_kernel<<<1, 1, 0, q>>>(hc, h->cgs);
+            ++kernels;
+            return cudaGetLastError() == cudaSuccess;
+        };
+        auto body = [&](cudaStream_t q, cudaGraphConditionalHandle hc) {
+            for (int it = 0; it < 2; ++it) {
+                cudaError_t e;
+                if (md.dir32) {
+                    EpiCG<float> ep{h->f_p, h->f_Db, h->f_q, h->ws(&h->cgs->pq), 0.0};
+                    e = solve_AtA32(h, h->f_p, ep, &h->cgs->done, q);
+                    if (e != cudaSuccess) return false;
+                    ew_launch(cg_update_kernel<float, float>, n, q, n, it, xf, h->f_r, h->f_p, h->f_q, Minv32,
+                              h->ws(h->slots + SL_DUMMY), h->cgs);
+                    ew_launch(cg_pupdate_kernel<float>, n, q, n, it, h->f_r, Minv32, h->f_p, h->cgs);
+                } else {
+                    EpiCG<double> ep{h->cg_p, h->Db, h->cg_q, h->ws(&h->cgs->pq), 0.0};
+                    e = solve_AtA(h, h->cg_p, ep, &h->cgs->done, q);
+                    if (e != cudaSuccess) return false;
+                    ew_launch(cg_update_kernel<double, double>, n, q, n, it, x, h->cg_r, h->cg_p, h->cg_q, Minv,
+                              h->ws(h->slots + SL_DUMMY), h->cgs);
+                    ew_launch(cg_pupdate_kernel<double>, n, q, n, it, h->cg_r, Minv, h->cg_p, h->cgs);
+                }
+            }
+            cg_continue_kernel<<<1, 1, 0, q>>>(hc, h->cgs, cap);
+            return cudaGetLastError() == cudaSuccess;
+        };
+        return capture_conditional(s, sb, cudaGraphCondTypeWhile, arm, body);
+    };
+    auto check = [&](int which, cudaGraphConditionalHandle hi, cudaStream_t q) {
+        ipm_cg_check_kernel<<<1, 1, 0, q>>>(h->cgs, h->ctl, which, cap_is_limit, hi, loop);
+        ++kernels;
+        return cudaGetLastError() == cudaSuccess;
+    };
+    if (ok) ok = cudaStreamBeginCaptureToGraph(ss[0], lp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        cudaStream_t s0 = ss[0];
+        // ---- predictor from zero: FP32 directions start from the residual
+        // pass's CG start, FP64 ones from r = rhs
+        if (!md.dir32) {
+            ew_launch(fill_kernel, n, s0, n, 0.0, h->dba);
+            ew_launch(cg_init_kernel<double>, n, s0, n, (const double*)h->rhs, (const double*)nullptr, 0, Minv,
+                      h->cg_r, h->cg_p, h->ws(h->slots + SL_DUMMY), h->cgs, 0.0, DevScalar(0.0, rt_dev));
+            kernels += 2;
+        } else {
+            ew_launch(fill_f32_kernel, n, s0, n, 0.0f, h->f_dba);
+            kernels += 1;
+        }
+        ok = cg_loop(s0, ss[4], h->dba, h->f_dba);
+        ok = ok && capture_conditional(
+                       s0, ss[1], cudaGraphCondTypeIf, [&](cudaStream_t q, cudaGraphConditionalHandle hi) { return check(1, hi, q); },
+                       [&](cudaStream_t s1, cudaGraphConditionalHandle) -> bool {
+                           // ---- corrector
+                           if (md.dir32)
+                               ew_launch(ipm_stepstats_kernel<float>, n, s1, n, h->lambda, h->s1, h->s2, h->z1, h->z2,
+                                         (const float*)nullptr, (const double*)nullptr, h->f_dba,
+                                         h->ws(h->slots + SL_SS));
+                           else
+                               ew_launch(ipm_stepstats_kernel<double>, n, s1, n, h->lambda, h->s1, h->s2, h->z1,
+                                         h->z2, (const double*)nullptr, (const double*)nullptr, h->dba,
+                                         h->ws(h->slots + SL_SS));
+                           ipm_sigma_kernel<<<1, 1, 0, s1>>>(h->slots + SL_SS, h->ctl, h->slots + SL_SIGMU);
+                           if (launch_corrector_rhs(h, s1, md, md.dir32 ? RESID_F32 : RESID_CG64, &h->ctl->rin) !=
+                               cudaSuccess)
+                               return false;
+                           kernels += 3;
+                           if (!md.dir32) {
+                               // r = rhs_c - K dba (written to rd by the rhs pass), from x = dba
+                               ew_launch(cg_init_kernel<double>, n, s1, n, (const double*)h->rd, (const double*)nullptr,
+                                         0, Minv, h->cg_r, h->cg_p, h->ws(h->slots + SL_DUMMY), h->cgs, 0.0,
+                                         DevScalar(0.0, rt_dev));
+                               ++kernels;
+                           }
+                           if (!cg_loop(s1, ss[4], h->db, h->f_db)) return false;
+                           return capture_conditional(
+                               s1, ss[2], cudaGraphCondTypeIf,
+                               [&](cudaStream_t q, cudaGraphConditionalHandle hi) { return check(2, hi, q); },
+                               [&](cudaStream_t s2, cudaGraphConditionalHandle) -> bool {
+                                   // ---- step, next product, next residual pass and stop test
+                                   if (launch_step(h, s2, md) != cudaSuccess) return false;
+                                   EpiStore<double> ep{h->Qb};
+                                   if (solve_AtA(h, h->beta, ep, nullptr, s2) != cudaSuccess) return false;
+                                   if (launch_resid_pass(h, s2, md, true, &h->ctl->rin_next) != cudaSuccess)
+                                       return false;
+                                   ipm_stop_kernel<<<1, 1, 0, s2>>>(h->slots + SL_RED, h->ctl, 1, loop);
+                                   kernels += 3 + passes_per_product(h->g) + 2;
+                                   return cudaGetLastError() == cudaSuccess;
+                               });
+                       });
+        cudaGraph_t out = nullptr;
+        ok = cudaStreamEndCapture(ss[0], &out) == cudaSuccess && ok;
+    }
+    if (ok) ok = cudaGraphInstantiate(&h->ipm_exec, graph, 0) == cudaSuccess;
+    for (auto& x : ss)
+        if (x) cudaStreamDestroy(x);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (!ok) h->ipm_exec = nullptr;
+    h->ipm_body_kernels = kernels;
+    return ok;
+}
+
+// Runs the iteration graph from the current iterate (its residual pass and
+// stop test done, the method still running).  Returns 0 with the control
+// block read back (status: stopped, or IPM_ABORT with the iteration handed
+// back), 1 when no graph could be built, or a (negative) csipm_status.
+int ipm_graph_run(csipm_handle h, const IpmMode& md, csipm_stats* S) {
+    if (!h->ipm_exec && !build_ipm_graph(h, md)) {
+        h->ipm_graph_off = true;
+        return 1;
+    }
+    cudaStream_t st = h->stream;
+    h->hctl->cg_iter = 0;
+    h->hctl->graph_iters = 0;
+    CK(cudaMemcpyAsync(&h->ctl->cg_iter, &h->hctl->cg_iter, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaGraphLaunch(h->ipm_exec, st));
+    CK(cudaMemcpyAsync(h->hctl, h->ctl, sizeof(IpmCtl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const IpmCtl& C = *h->hctl;
+    S->cg_iter += C.cg_iter;
+    S->graph_iters += C.graph_iters;
+    // one product per CG iteration plus the residual product of every completed body
+    h->matvecs += C.cg_iter + C.graph_iters;
+    const int ppp = passes_per_product(h->g);
+    h->launches += 1 + (long long)C.graph_iters * h->ipm_body_kernels + (long long)C.cg_iter * (ppp + 2) +
+                   (C.cg_iter + 1) / 2;
+    return CSIPM_OK;
+}
+
 }  // namespace csipm_internal
 
 extern "C" {
@@ -536,6 +851,7 @@ int csipm_default_options(csipm_options* opt) {
     opt->cuda_graphs = 1;
     opt->autotune = 1;
     opt->stream = nullptr;
+    opt->ipm_cg_forcing = 100.0;
     return CSIPM_OK;
 }
 
@@ -615,7 +931,8 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s3_cfg.grid.x * h->op64.s3_cfg.grid.y);
     const size_t n_ = (size_t)h->N;
     if (!h->alloc(&h->partials, maxblocks * 8) || !h->alloc(&h->ticket, 1) || !h->alloc(&h->slots, SL_COUNT) ||
-        !h->alloc(&h->cgs, 1) || !h->alloc(&h->b, n_) || !h->alloc(&h->beta, n_) || !h->alloc(&h->c, n_) ||
+        !h->alloc(&h->cgs, 1) || !h->alloc(&h->ctl, 1) || !h->alloc(&h->b, n_) || !h->alloc(&h->beta, n_) ||
+        !h->alloc(&h->c, n_) ||
         !h->alloc(&h->s1, n_) || !h->alloc(&h->s2, n_) ||
         !h->alloc(&h->z1, n_) || !h->alloc(&h->z2, n_) || !h->alloc(&h->Qb, n_) || !h->alloc(&h->rd, n_) ||
         !h->alloc(&h->Db, n_) || !h->alloc(&h->Minv, n_) || !h->alloc(&h->rhs, n_) || !h->alloc(&h->dba, n_) ||
@@ -627,9 +944,11 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         return bail(CSIPM_ERR_OOM, h->err);
     static_assert(sizeof(double) * SL_COUNT == csipm_handle_s::HSLOT_BYTES, "slot block size");
     static_assert(sizeof(CgScalars) <= csipm_handle_s::HCGS_BYTES, "CG scalar block size");
+    static_assert(sizeof(IpmCtl) <= csipm_handle_s::HCTL_BYTES, "IPM control block size");
     h->hslots = (double*)pinned_get(csipm_handle_s::HSLOT_BYTES);
     h->hcgs = (CgScalars*)pinned_get(csipm_handle_s::HCGS_BYTES);
-    if (!h->hslots || !h->hcgs) return bail(CSIPM_ERR_OOM, "pinned host allocation failed");
+    h->hctl = (IpmCtl*)pinned_get(csipm_handle_s::HCTL_BYTES);
+    if (!h->hslots || !h->hcgs || !h->hctl) return bail(CSIPM_ERR_OOM, "pinned host allocation failed");
     cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int), h->stream);
     cudaMemsetAsync(h->slots, 0, sizeof(double) * SL_COUNT, h->stream);
     cudaEventCreate(&h->ev0);
@@ -745,17 +1064,9 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     const long long la0 = h->launches;
     const bool mixed = o.precision == CSIPM_MIXED;
     const int ppp = passes_per_product(h->g);
-    // mixed precision with a Newton tolerance the FP32 warm start serves:
-    // the FP64 barrier diagonals are only computed when a solve needs them
-    const bool lazy64 = mixed && o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL;
-    // the same loose mode keeps the Newton directions in FP32 (f_dba, f_db):
-    // they are only asked to a relative accuracy >= 1e-4, far above FP32
-    // rounding, and the IPM residual is recomputed in FP64 every iteration
-    const bool dir32 = lazy64;
-    // relative tolerance of round 0 of a mixed Newton solve (schur_mixed)
-    const double cg_rin = std::max(o.ipm_cg_rtol, MIXED_INNER_RTOL);
+    const IpmMode md = ipm_mode(h);
+    const bool lazy64 = md.lazy64, dir32 = md.dir32;
     cudaEventRecord(h->ev0, st);
-    // every beta-space vector of the solve is in solver order when h->sorder
     const double* bv = h->sorder ? h->bs : h->b;
     // ---- initial point: beta = soft(A^T z0, lambda), z from the clipped gradient, c balanced
     ew_launch(ipm_init1_kernel, n, st, n, bv, lam, h->beta, h->ws(h->slots + SL_MAXB));
@@ -773,19 +1084,41 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         int r0 = read_slots(h, SL_MAXB, 2);
         if (r0) return r0;
     }
-    const double kkt_scale = std::max(1.0, h->hslots[SL_MAXB + 1]);
+    // ---- the device control block: stop test and Newton tolerances
+    {
+        IpmCtl& c = *h->hctl;
+        std::memset(&c, 0, sizeof(IpmCtl));
+        c.tol = o.tol;
+        c.rt_opt = o.ipm_cg_rtol;
+        c.forcing = o.ipm_cg_forcing;
+        c.rt_floor = CG_FORCING_FLOOR;
+        c.rin_floor = MIXED_INNER_RTOL;
+        c.z0sq = h->z0sq;
+        c.kkt_scale = std::max(1.0, h->hslots[SL_MAXB + 1]);
+        c.lam = lam;
+        c.two_n = 2.0 * (double)n;
+        c.max_iter = o.max_iter;
+        c.k = -1;
+        c.rt_next = o.ipm_cg_rtol;   // iteration 0 solves at the option
+        c.rin_next = std::max(o.ipm_cg_rtol, MIXED_INNER_RTOL);
+        c.status = IPM_RUNNING;
+        CK(cudaMemcpyAsync(h->ctl, h->hctl, sizeof(IpmCtl), cudaMemcpyHostToDevice, st));
+    }
+    const double* rt_dev = &h->ctl->rt;
+    const double* rin_dev = &h->ctl->rin;
     int status = CSIPM_ERR_IPM_MAXITER;
-    double mu = 0.0, gap = 1.0;
-    int k = 0;
-    for (;; ++k) {
-        if (k > 0) {
+    bool pending = false;    // a beta step whose slack / multiplier step waits for the next residual pass
+    bool qb_valid = true;    // Qb = A'A beta of the current beta (the initial point's product)
+    bool resume = false;     // a graph replay handed an iteration back: rerun its residual pass only
+    bool use_graph = md.graphable && !h->ipm_graph_off;
+    for (;;) {
+        if (!qb_valid) {
             EpiStore<double> ep{h->Qb};
             CK(solve_AtA(h, h->beta, ep, nullptr, st));
             h->matvecs++;
             h->launches += ppp;
         }
-        h->launches += 1;   // pending s/z step + residual + barrier diagonals + predictor right-hand side
-        const bool step = k > 0;
+        qb_valid = false;
         h->diag64_stale = lazy64;
         {
             // algorithmic bytes: b, Qb, beta, s1, s2, z1, z2 read; rd, rhs written;
@@ -793,123 +1126,102 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
             // the barrier diagonals written in FP64 and/or FP32; with FP32
             // directions the predictor CG's r and p written
             const double td = dir32 ? 4.0 : 8.0;
-            const double per = 56.0 + 16.0 + (step ? 2.0 * td + 32.0 : 0.0) + (lazy64 ? 0.0 : 16.0) +
+            const double per = 56.0 + 16.0 + (pending ? 2.0 * td + 32.0 : 0.0) + (lazy64 ? 0.0 : 16.0) +
                                (mixed ? 8.0 : 0.0) + (dir32 ? 8.0 : 0.0);
             S.resid_pass_bytes += per * (double)n;
             S.resid_pass_launches += 1;
         }
         cudaEventRecord(h->ev_rp[0], st);
-        if (dir32)
-            ew_launch(ipm_resdiag_kernel<float, float>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1, h->z2,
-                      step ? h->f_dba : nullptr, step ? h->f_db : nullptr, h->slots + SL_SIGMU, h->slots + SL_ALPHA,
-                      h->rd, (double*)nullptr, (double*)nullptr, h->f_Db, h->f_Minv, o.preconditioner, h->rhs,
-                      h->ws(h->slots + SL_RED), h->f_r, h->f_p, h->cgs, cg_rin);
-        else
-            ew_launch(ipm_resdiag_kernel<float, double>, n, st, n, bv, h->Qb, lam, h->beta, h->s1, h->s2, h->z1,
-                      h->z2, step ? h->dba : nullptr, step ? h->db : nullptr, h->slots + SL_SIGMU,
-                      h->slots + SL_ALPHA, h->rd, lazy64 ? nullptr : h->Db, lazy64 ? nullptr : h->Minv,
-                      mixed ? h->f_Db : nullptr, mixed ? h->f_Minv : nullptr, o.preconditioner, h->rhs,
-                      h->ws(h->slots + SL_RED), (float*)nullptr, (float*)nullptr, (CgScalars*)nullptr, 0.0);
-        CK(cudaGetLastError());
+        // a resumed iteration restarts its predictor at this iteration's tolerance
+        CK(launch_resid_pass(h, st, md, pending, resume ? rin_dev : &h->ctl->rin_next));
         cudaEventRecord(h->ev_rp[1], st);
-        int r = read_slots(h, SL_RED, RR_N);
-        if (r) return r;
+        pending = false;
+        h->launches += 1;
+        if (!resume) {
+            ipm_stop_kernel<<<1, 1, 0, st>>>(h->slots + SL_RED, h->ctl, 0, 0);
+            CK(cudaGetLastError());
+            h->launches += 1;
+        }
+        resume = false;
+        CK(cudaMemcpyAsync(h->hctl, h->ctl, sizeof(IpmCtl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
         {
             float rp_ms = 0.f;   // the stream is synchronised: both events are complete
             if (cudaEventElapsedTime(&rp_ms, h->ev_rp[0], h->ev_rp[1]) == cudaSuccess) S.resid_pass_ms += rp_ms;
         }
-        const double* R = h->hslots + SL_RED;
-        mu = R[RR_SZ] / (2.0 * (double)n);
-        const double usq = h->z0sq - 2.0 * R[RR_BB] + R[RR_BQB];
-        const double F = 0.5 * usq + lam * R[RR_L1];
-        const double th = R[RR_GINF] > 0.0 ? std::min(1.0, lam / R[RR_GINF]) : 1.0;
-        const double D = th * (h->z0sq - R[RR_BB]) - 0.5 * th * th * usq;
-        gap = (F - D) / std::max(std::fabs(F), 1e-300);
-        // scaled KKT error: the criterion that still applies when lambda = 0
-        // makes the LASSO dual bound degenerate
-        const double kkt = std::max(std::max(R[RR_RDINF], R[RR_RCINF]) / kkt_scale, R[RR_SZ] / std::max(1.0, std::fabs(F)));
-        S.obj = 0.5 * R[RR_BQB] - R[RR_BB] + lam * R[RR_SUMC];
-        S.lasso_obj = F;
-        S.dual_inf = R[RR_RDINF];
-        S.mu = mu;
-        S.gap = gap;
-        if (!std::isfinite(mu) || !std::isfinite(gap)) { status = fail(h, CSIPM_ERR_NONFINITE, "non-finite iterate"); break; }
+        const IpmCtl& C = *h->hctl;
         if (o.verbose)
-            std::fprintf(stderr, "csipm it %3d  mu %.3e  gap %.3e  |rd| %.2e  |rc| %.2e  obj %.12e  cg %d\n", k, mu, gap,
-                         R[RR_RDINF], R[RR_RCINF], F, S.cg_iter);
-        if (gap <= o.tol || kkt <= o.tol) { status = CSIPM_OK; break; }
-        if (k >= o.max_iter) { status = CSIPM_ERR_IPM_MAXITER; break; }
+            std::fprintf(stderr, "csipm it %3d  mu %.3e  gap %.3e  |rd| %.2e  obj %.12e  rtol %.1e  cg %d\n", C.k, C.mu,
+                         C.gap, C.dual_inf, C.F, C.rt, S.cg_iter);
+        if (C.status != IPM_RUNNING) break;
+        if (use_graph) {
+            // every further iteration inside one graph launch: no host round trip
+            // until the method stops or a Newton solve needs the host
+            const int g = ipm_graph_run(h, md, &S);
+            if (g == 1) {   // the graph could not be built: plain launches from here on
+                use_graph = false;
+            } else if (g) {
+                return g;
+            } else if (h->hctl->status == IPM_ABORT) {
+                use_graph = false;
+                resume = true;       // Qb is current and no step is pending
+                qb_valid = true;
+                h->hctl->status = IPM_RUNNING;
+                CK(cudaMemcpyAsync(&h->ctl->status, &h->hctl->status, sizeof(int), cudaMemcpyHostToDevice, st));
+                continue;
+            } else {
+                break;
+            }
+        }
+        const double rt = C.rt;                               // this iteration's Newton tolerance (host copy)
+        const double cg_rin = C.rin;
         // ---- predictor (affine scaling): diagonals and right-hand side came with the residual
         int its = 0;
-        int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its, nullptr,
-                                     dir32 ? h->f_dba : nullptr, dir32)
-                       : schur_cg(h, h->rhs, h->dba, false, o.ipm_cg_rtol, o.cg_maxit, &its);
+        int cs = mixed ? schur_mixed(h, h->rhs, h->dba, false, rt, o.cg_maxit, &its, nullptr,
+                                     dir32 ? h->f_dba : nullptr, dir32, rin_dev)
+                       : schur_cg(h, h->rhs, h->dba, false, rt, o.cg_maxit, &its, nullptr, rt_dev);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
         // the centring target and the step length are computed on the device
         // from the step statistics: no host round trip inside the iteration
-        double* sigmu_d = h->slots + SL_SIGMU;
-        double* alpha_d = h->slots + SL_ALPHA;
         if (dir32)
             ew_launch(ipm_stepstats_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, (const float*)nullptr,
                       (const double*)nullptr, h->f_dba, h->ws(h->slots + SL_SS));
         else
             ew_launch(ipm_stepstats_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
                       (const double*)nullptr, (const double*)nullptr, h->dba, h->ws(h->slots + SL_SS));
-        ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, mu, 2.0 * (double)n, sigmu_d);
+        ipm_sigma_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, h->ctl, h->slots + SL_SIGMU);
         // ---- corrector, warm-started at dba.  Its starting residual
         // rhs_c - K dba = rhs_c - rhs_p + (rhs_p - K dba) comes from the
         // predictor solve's residual (kept by CG's recurrence) with no
         // product; mixed precision at tight Newton tolerances computes it
         // with an FP64 product instead, as refinement wants.
         const int rk = (!mixed || o.ipm_cg_rtol >= MIXED_FP32_WARM_RTOL) ? h->resid_kind : RESID_NONE;
-        const float* rp32 = rk == RESID_F32 ? h->f_r : nullptr;
-        const double* rp64 = rk == RESID_CG64 ? h->cg_r : nullptr;
-        // FP32 directions with a known warm-start residual: this pass also
-        // starts the corrector's FP32 CG (r, p, scalars), replacing its init pass
+        CK(launch_corrector_rhs(h, st, md, rk, rin_dev));
         const bool cstart = dir32 && rk != RESID_NONE;
-        float* cr = cstart ? h->f_r : nullptr;
-        float* cp = cstart ? h->f_p : nullptr;
-        const float* cm = o.preconditioner ? h->f_Minv : nullptr;
-        RedWorkspace cws = h->ws(h->slots + SL_DUMMY);
-        if (dir32 && rp32)
-            ew_launch(ipm_rhs_kernel<float, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp32, h->f_db, cr, cp, cm, h->cgs, cws,
-                      cg_rin);
-        else if (dir32)
-            ew_launch(ipm_rhs_kernel<double, float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const float*)h->f_dba, (const double*)sigmu_d, h->rhs, rp64, h->f_db, cr, cp, cm, h->cgs, cws,
-                      cg_rin);
-        else if (rp32)
-            ew_launch(ipm_rhs_kernel<float, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp32, h->db, (float*)nullptr,
-                      (float*)nullptr, (const float*)nullptr, (CgScalars*)nullptr, cws, 0.0);
-        else
-            ew_launch(ipm_rhs_kernel<double, double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2, h->rd,
-                      (const double*)h->dba, (const double*)sigmu_d, h->rhs, rp64, h->db, (float*)nullptr,
-                      (float*)nullptr, (const float*)nullptr, (CgScalars*)nullptr, cws, 0.0);
-        CK(cudaGetLastError());
         const double* r0v = rk != RESID_NONE && !cstart ? h->rd : nullptr;
-        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v,
-                                 dir32 ? h->f_db : nullptr, cstart)
-                   : schur_cg(h, h->rhs, h->db, true, o.ipm_cg_rtol, o.cg_maxit, &its, r0v);
+        cs = mixed ? schur_mixed(h, h->rhs, h->db, true, rt, o.cg_maxit, &its, r0v, dir32 ? h->f_db : nullptr,
+                                 cstart, rin_dev)
+                   : schur_cg(h, h->rhs, h->db, true, rt, o.cg_maxit, &its, r0v, rt_dev);
         S.cg_iter += its;
         if (cs != CSIPM_OK && cs != CSIPM_ERR_CG_MAXITER) { status = cs; break; }
-        if (dir32)
-            ew_launch(ipm_stepstats_kernel<float>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
-                      (const float*)h->f_dba, (const double*)sigmu_d, (const float*)h->f_db, h->ws(h->slots + SL_SS));
-        else
-            ew_launch(ipm_stepstats_kernel<double>, n, st, n, lam, h->s1, h->s2, h->z1, h->z2,
-                      (const double*)h->dba, (const double*)sigmu_d, (const double*)h->db, h->ws(h->slots + SL_SS));
-        ipm_alpha_kernel<<<1, 1, 0, st>>>(h->slots + SL_SS, std::max(0.99, 1.0 - mu), alpha_d);
-        // beta steps now (the next A'A product needs it); s and z take the
-        // same step inside the next residual pass
-        if (dir32)
-            ew_launch(ipm_beta_step_kernel<float>, n, st, n, h->beta, (const float*)h->f_db, (const double*)alpha_d);
-        else
-            ew_launch(ipm_beta_step_kernel<double>, n, st, n, h->beta, (const double*)h->db, (const double*)alpha_d);
-        CK(cudaGetLastError());
+        (void)cg_rin;
+        CK(launch_step(h, st, md));
         h->launches += 6;   // sigma, corrector rhs, 2 step statistics, alpha, beta step (+ the Newton solves' launches)
+        pending = true;
+    }
+    {
+        const IpmCtl& C = *h->hctl;
+        if (status == CSIPM_ERR_IPM_MAXITER) {   // no solver error: the control block says why the loop ended
+            if (C.status == IPM_CONVERGED) status = CSIPM_OK;
+            else if (C.status == IPM_NONFINITE) status = fail(h, CSIPM_ERR_NONFINITE, "non-finite iterate");
+        }
+        S.obj = C.obj;
+        S.lasso_obj = C.F;
+        S.dual_inf = C.dual_inf;
+        S.mu = C.mu;
+        S.gap = C.gap;
+        S.ipm_iter = C.k;
     }
     if (c_out) {
         ew_launch(half_sum_kernel, n, st, n, h->s1, h->s2, h->c);
@@ -930,7 +1242,6 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     S.solve_ms = ms;
     S.status = status;
-    S.ipm_iter = k;
     S.matvecs = h->matvecs - mv0;
     S.refinements = h->refinements - rf0;
     S.fallbacks = h->fallbacks - fb0;

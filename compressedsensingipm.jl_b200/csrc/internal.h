@@ -135,6 +135,13 @@ struct csipm_handle_s {
     cudaGraphExec_t cg_exec64[2] = {nullptr, nullptr};
     cudaGraphExec_t cg_exec32[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t admm_exec[2] = {nullptr, nullptr};   // ADMM x-update CG, one per x buffer
+    // csipm_solve's device control block (stop test, tolerances) and the
+    // graph of whole interior-point iterations, captured on first use
+    IpmCtl* ctl = nullptr;
+    IpmCtl* hctl = nullptr;         // pinned host mirror
+    cudaGraphExec_t ipm_exec = nullptr;
+    int ipm_body_kernels = 0;       // kernels of one graph iteration outside its CG loops
+    bool ipm_graph_off = false;     // its capture failed: csipm_solve runs plain iterations
     bool graphs_off = false;        // a capture failed: plain launches
     bool diag64_stale = false;      // FP64 Db/Minv not yet computed for this iterate (mixed precision)
     int resid_kind = 0;             // where the last Newton solve left rhs - K x (RESID_*)
@@ -150,6 +157,7 @@ struct csipm_handle_s {
     cudaMemPool_t pool = nullptr;   // device_pool(device): every device buffer of the handle
     static constexpr size_t HSLOT_BYTES = sizeof(double) * 64;   // SL_COUNT slots
     static constexpr size_t HCGS_BYTES = 64;                     // >= sizeof(CgScalars)
+    static constexpr size_t HCTL_BYTES = 256;                    // >= sizeof(IpmCtl)
 
     ~csipm_handle_s() {
         for (auto& g : cg_exec64)
@@ -158,6 +166,8 @@ struct csipm_handle_s {
             if (g) cudaGraphExecDestroy(g);
         for (auto& g : admm_exec)
             if (g) cudaGraphExecDestroy(g);
+        if (ipm_exec) cudaGraphExecDestroy(ipm_exec);
+        if (hctl) pinned_put(hctl, HCTL_BYTES);
         for (void* p : allocs) cudaFreeAsync(p, stream);
         allocs.clear();
         op64.release();
@@ -390,10 +400,14 @@ enum { RESID_NONE = 0, RESID_CG64 = 1, RESID_F32 = 2 };   // none / FP64 in cg_r
 // wrote the FP32 CG start (f_r, f_p, h->cgs) for round 0.  On return
 // h->resid_kind says where the residual
 // rhs - K x of the result is held (RESID_*).
+// rtol_dev (optional): the device copy of rtol the CG thresholds are read
+// from (csipm_solve's control block: plain launches then read the same value
+// graph replays do); rin_dev likewise for round 0 of a mixed solve.
 int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-             const double* r0v = nullptr);
+             const double* r0v = nullptr, const double* rtol_dev = nullptr);
 int schur_mixed(csipm_handle h, const double* rhs, double* x, bool has_x0, double rtol, int maxit, int* iters,
-                const double* r0v = nullptr, float* xf = nullptr, bool ready = false);
+                const double* r0v = nullptr, float* xf = nullptr, bool ready = false,
+                const double* rin_dev = nullptr);
 int ensure_kkt_buffers(csipm_handle h);
 int ensure_gondzio_buffers(csipm_handle h);
 

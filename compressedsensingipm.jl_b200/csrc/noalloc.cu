@@ -9,8 +9,8 @@
 // — in one file-scope device array of fixed size.  Every GPU that loads the
 // library holds the array until the process exits; all calls share it, so
 // calls that overlap on the GPU race, and each call rewrites everything it
-// reads (the gather pass writes the whole spectrum, the twiddles are copied
-// in on every call).
+// reads: a small kernel writes the twiddle tables for the call's sizes (no
+// host-to-device copy) and the first pass writes the whole spectrum.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -20,6 +20,7 @@
 
 #include "../../include/csipm.h"
 #include "geometry.h"
+#include "long1d.cuh"
 #include "operator.cuh"
 
 using namespace csipm;
@@ -63,6 +64,25 @@ int scratch_address(void** out) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// W_L^e = exp(-2 pi i e / L), e < L, written on the device: sincospi of the
+// exactly reduced angle 2e/L in [0, 2) (one rounding of the quotient, then
+// CUDA's sincospi), so no host table is copied per call.  The handle path's
+// tables are rounded from long double; these agree with them to an ulp or
+// two, far inside the operator's 1e-12 tolerance.
+__global__ void static_twiddle_kernel(int L, double2* __restrict__ out) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < L; e += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi((double)(2 * (long long)e) / (double)L, &s, &c);
+        out[e] = make_double2(c, -s);
+    }
+}
+
+cudaError_t put_twiddles(int L, double2* dst, cudaStream_t st) {
+    const int blocks = (L + 255) / 256 < 1024 ? (L + 255) / 256 : 1024;
+    static_twiddle_kernel<<<blocks, 256, 0, st>>>(L, dst);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 extern "C" {
@@ -77,11 +97,41 @@ int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, 
     if ((long long)n[0] * n[1] * n[2] >= (1LL << 31)) return static_fail(CSIPM_ERR_UNSUPPORTED, "N must be below 2^31");
     const Geom g = make_geom(dim, n, n[0] / 2 + 1);
     using C = double2;
+
+    // operator description over the static scratch (no allocation anywhere):
+    // plans and pass configurations first, then the carve-up of the array
+    FftOperator<double> op;
+    op.owns = false;
+    op.g = g;
+    op.stream = (cudaStream_t)stream;
+    std::string err;
+    const bool long1d = dim == 1 && g.m1 > L1D_MIN_M;   // the handle path's four-step rows
+    if (long1d) {
+        if (!l1d_split(g.m1, &op.l1P, &op.l1Q))
+            return static_fail(CSIPM_ERR_UNSUPPORTED, "1D length has no split M = P*Q with P <= 4096, Q <= 768");
+        if (!make_fft_plan(op.l1P, &op.planP, &err, op.max_radix()) ||
+            !make_fft_plan(op.l1Q, &op.planQ, &err, op.max_radix()))
+            return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+        if (!op.choose_strided(op.planQ, op.l1Q, op.l1P, 1, &op.q_cfg, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+        op.l1RB = 1;
+        while (op.l1RB < 16 && 2 * (size_t)op.l1P * (2 * op.l1RB) * sizeof(C) <= 96 * 1024) op.l1RB *= 2;
+        op.plan1 = op.planP;
+    } else {
+        if (!op.make_plans(&err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+        if (!op.choose_row(g.n2 * g.n3, &op.row_cfg, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+    }
+    if (dim >= 2 && !op.choose_strided(op.plan2, g.n2, g.m1 + 1, dim == 3 ? g.n3 : 1, &op.s2_cfg, &err))
+        return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+    if (dim >= 3 && !op.choose_strided(op.plan3, g.n3, g.m1 + 1, g.n2, &op.s3_cfg, &err))
+        return static_fail(CSIPM_ERR_UNSUPPORTED, err);
+
     const size_t spec_b = align256(sizeof(C) * (size_t)g.ld1 * g.n2 * g.n3);
     const size_t tw1_b = align256(sizeof(C) * (size_t)g.n1);
     const size_t tw2_b = dim >= 2 ? align256(sizeof(C) * (size_t)g.n2) : 0;
     const size_t tw3_b = dim >= 3 ? align256(sizeof(C) * (size_t)g.n3) : 0;
-    const size_t need = spec_b + tw1_b + tw2_b + tw3_b;
+    const size_t twP_b = long1d ? align256(sizeof(C) * (size_t)op.l1P) : 0;
+    const size_t twQ_b = long1d ? align256(sizeof(C) * (size_t)op.l1Q) : 0;
+    const size_t need = spec_b + tw1_b + tw2_b + tw3_b + twP_b + twQ_b;
     if (need > STATIC_SCRATCH_BYTES)
         return static_fail(CSIPM_ERR_UNSUPPORTED, "problem needs " + std::to_string(need) +
                                                       " bytes of scratch; csipm_apply_AtA_static holds at most " +
@@ -90,47 +140,41 @@ int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, 
     int st = scratch_address(&base);
     if (st) return st;
     unsigned char* p = static_cast<unsigned char*>(base);
-
-    // operator description over the static scratch (no allocation anywhere)
-    FftOperator<double> op;
-    op.owns = false;
-    op.g = g;
-    op.stream = (cudaStream_t)stream;
-    std::string err;
-    if (!op.make_plans(&err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    if (!op.choose_row(g.n2 * g.n3, &op.row_cfg, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    if (dim >= 2 && !op.choose_strided(op.plan2, g.n2, g.m1 + 1, dim == 3 ? g.n3 : 1, &op.s2_cfg, &err))
-        return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    if (dim >= 3 && !op.choose_strided(op.plan3, g.n3, g.m1 + 1, g.n2, &op.s3_cfg, &err))
-        return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-    op.spec = reinterpret_cast<C*>(p);
-    op.tw1 = reinterpret_cast<C*>(p + spec_b);
-    op.tw2 = dim >= 2 ? reinterpret_cast<C*>(p + spec_b + tw1_b) : nullptr;
-    op.tw3 = dim >= 3 ? reinterpret_cast<C*>(p + spec_b + tw1_b + tw2_b) : nullptr;
+    size_t off = 0;
+    auto carve = [&](size_t b) { C* q = b ? reinterpret_cast<C*>(p + off) : nullptr; off += b; return q; };
+    op.spec = carve(spec_b);
+    op.tw1 = carve(tw1_b);
+    op.tw2 = carve(tw2_b);
+    op.tw3 = carve(tw3_b);
+    op.twP = carve(twP_b);
+    op.twQ = carve(twQ_b);
     op.maskw = const_cast<uint32_t*>(keep_bits);   // read-only in every pass
     op.wpr = (g.n1 + 31) / 32;
 
-    // twiddle tables: rewritten on every call (the array keeps the last call's contents)
+    // twiddle tables of this call's sizes (the array keeps the last call's contents)
     cudaStream_t s = (cudaStream_t)stream;
-    auto put_table = [&](int L, C* dst) -> int {
-        std::vector<double> t;
-        twiddle_table(L, &t);
-        cudaError_t e = cudaMemcpyAsync(dst, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return static_fail(CSIPM_ERR_CUDA, std::string("twiddle copy: ") + cudaGetErrorString(e));
-        return CSIPM_OK;
-    };
-    if ((st = put_table(g.n1, op.tw1))) return st;
-    if (dim >= 2 && (st = put_table(g.n2, op.tw2))) return st;
-    if (dim >= 3 && (st = put_table(g.n3, op.tw3))) return st;
+    cudaError_t e = put_twiddles(g.n1, op.tw1, s);
+    if (e == cudaSuccess && dim >= 2) e = put_twiddles(g.n2, op.tw2, s);
+    if (e == cudaSuccess && dim >= 3) e = put_twiddles(g.n3, op.tw3, s);
+    if (e == cudaSuccess && long1d) e = put_twiddles(op.l1P, op.twP, s);
+    if (e == cudaSuccess && long1d) e = put_twiddles(op.l1Q, op.twQ, s);
+    if (e != cudaSuccess) return static_fail(CSIPM_ERR_CUDA, std::string("twiddle kernel: ") + cudaGetErrorString(e));
 
-    // the five (3D) / three (2D) / one (1D) fused passes of A^T A
+    // the fused passes of A^T A: five (3D), three (2D), one row pass (1D) or
+    // the four passes of a long 1D row
     const double sc = 1.0 / (2.0 * (double)g.N);
     const bool mask = keep_bits != nullptr;
     EpiStore<double> none{nullptr};
     EpiStore<double> out{y};
     PassArgs<double> ra = op.row_args(sc, nullptr, nullptr);
-    cudaError_t e = cudaSuccess;
-    if (dim == 1) {
+    if (long1d) {
+        e = l1d_first(op, x, nullptr, s);
+        if (e == cudaSuccess)
+            e = mask ? l1d_row<double, IN_SPEC, OUT_SPEC, true>(op, sc, nullptr, nullptr, nullptr, s)
+                     : l1d_row<double, IN_SPEC, OUT_SPEC, false>(op, sc, nullptr, nullptr, nullptr, s);
+        if (e == cudaSuccess) e = l1d_lines_forward(op, nullptr, s);
+        if (e == cudaSuccess) e = l1d_post(op, out, nullptr, s);
+    } else if (dim == 1) {
         e = mask ? launch_row<double, IN_GATHER, OUT_SCATTER, true>(op.row_cfg, ra, x, out, s)
                  : launch_row<double, IN_GATHER, OUT_SCATTER, false>(op.row_cfg, ra, x, out, s);
     } else {

@@ -38,6 +38,7 @@ struct Pending {
 struct csipm_server_s {
     int device = 0;
     int slots = 0;
+    int cuda_graphs = 0;
     size_t budget = 0;
     size_t in_use = 0;
     bool stopping = false;
@@ -98,12 +99,39 @@ bool csipm_server_s::take(Pending* out) {
     return false;
 }
 
+// A slot's pinned host staging buffer for z0 and beta: copies from and to
+// pinned memory run asynchronously on the slot's stream (a pageable copy
+// would hold the slot's thread until the driver has staged it).  It grows in
+// powers of two and is handed back to the process-wide pinned free list.
+struct PinnedStage {
+    double* p = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t need) {
+        if (need <= bytes) return true;
+        size_t b = 1 << 16;
+        while (b < need) b <<= 1;
+        if (p) pinned_put(p, bytes);
+        p = static_cast<double*>(pinned_get(b));
+        bytes = p ? b : 0;
+        return p != nullptr;
+    }
+    ~PinnedStage() {
+        if (p) pinned_put(p, bytes);
+    }
+};
+
+static void set_message(csipm_result* r, const char* msg) {
+    std::strncpy(r->message, msg ? msg : "", sizeof(r->message) - 1);
+    r->message[sizeof(r->message) - 1] = 0;
+}
+
 void csipm_server_s::work(int slot) {
     (void)slot;
     cudaSetDevice(device);
     cudaStream_t st = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     cudaMemPool_t pool = device_pool(device);
+    PinnedStage stage;
     for (;;) {
         Pending p{};
         bool got = false;
@@ -125,33 +153,54 @@ void csipm_server_s::work(int slot) {
         double* z0 = nullptr;
         double* beta = nullptr;
         int status = CSIPM_OK;
+        const char* msg = nullptr;
+        std::string err;
         if (!pool || cudaMallocFromPoolAsync((void**)&z0, sizeof(double) * n, pool, st) != cudaSuccess ||
             cudaMallocFromPoolAsync((void**)&beta, sizeof(double) * n, pool, st) != cudaSuccess) {
             status = CSIPM_ERR_OOM;
+            msg = "out of device memory (staging z0 / beta)";
+        }
+        if (status == CSIPM_OK && !stage.ensure(sizeof(double) * (size_t)n)) {
+            status = CSIPM_ERR_OOM;
+            msg = "pinned host allocation failed";
         }
         csipm_handle h = nullptr;
-        if (status == CSIPM_OK && cudaMemcpyAsync(z0, pr.z0, sizeof(double) * n, cudaMemcpyHostToDevice, st) != cudaSuccess)
-            status = CSIPM_ERR_CUDA;
+        if (status == CSIPM_OK) {
+            std::memcpy(stage.p, pr.z0, sizeof(double) * (size_t)n);
+            if (cudaMemcpyAsync(z0, stage.p, sizeof(double) * n, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                status = CSIPM_ERR_CUDA;
+                msg = "z0 upload failed";
+            }
+        }
         if (status == CSIPM_OK) {
             csipm_problem dp = pr;
             dp.z0 = z0;
             csipm_options o = p.req.options;
             o.stream = st;
-            // a served handle lives for one solve: instantiating its CG-loop
-            // graphs on the slot threads costs more host time than the
-            // replays save (16 slots: 274 -> 352 solves/s without them)
-            o.cuda_graphs = 0;
+            // a served handle lives for one solve: its graphs are captured
+            // for that one solve, which pays off on the server's say-so only
+            o.cuda_graphs = cuda_graphs;
             status = csipm_create(&dp, &o, &h);
+            if (status != CSIPM_OK) err = csipm_last_error(nullptr);
         }
         if (status == CSIPM_OK) {
             status = csipm_solve(h, beta, nullptr, &res.stats);
+            if (status != CSIPM_OK) err = h->err;
             if (status == CSIPM_OK || status == CSIPM_ERR_IPM_MAXITER || status == CSIPM_ERR_CG_MAXITER) {
                 if (p.req.beta_out &&
-                    cudaMemcpyAsync(p.req.beta_out, beta, sizeof(double) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                    cudaMemcpyAsync(stage.p, beta, sizeof(double) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
                     status = CSIPM_ERR_CUDA;
-                if (cudaStreamSynchronize(st) != cudaSuccess) status = CSIPM_ERR_CUDA;
+                    msg = "beta download failed";
+                }
+                if (cudaStreamSynchronize(st) != cudaSuccess) {
+                    status = CSIPM_ERR_CUDA;
+                    msg = "stream synchronisation failed";
+                }
+                if (status != CSIPM_ERR_CUDA && p.req.beta_out)
+                    std::memcpy(p.req.beta_out, stage.p, sizeof(double) * (size_t)n);
             }
         }
+        if (status != CSIPM_OK) set_message(&res, msg ? msg : err.c_str());
         if (h) csipm_destroy(h);
         if (z0) cudaFreeAsync(z0, st);
         if (beta) cudaFreeAsync(beta, st);
@@ -190,6 +239,7 @@ int csipm_server_create(const csipm_server_options* opt, csipm_server* out) {
     auto* s = new csipm_server_s();
     s->device = dev;
     s->slots = opt && opt->slots > 0 ? opt->slots : 8;
+    s->cuda_graphs = opt && opt->cuda_graphs ? 1 : 0;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = opt && opt->hbm_budget > 0 ? opt->hbm_budget : (size_t)(0.8 * (double)free_b);

@@ -23,6 +23,16 @@ namespace csipm {
 
 constexpr int EW_THREADS = 256;
 
+// A kernel scalar given by value or read from device memory when the kernel
+// runs (the interior-point solve keeps its per-iteration Newton tolerance on
+// the device, so plain launches and graph replays read the same value).
+struct DevScalar {
+    double v;
+    const double* p;
+    __host__ __device__ DevScalar(double x = 0.0, const double* q = nullptr) : v(x), p(q) {}
+    __device__ __forceinline__ double get() const { return p ? *p : v; }
+};
+
 // ------------------------------------------------------------------ CG scalars
 // Device scalar block of one CG solve.  rz is double-buffered by iteration parity.
 struct CgScalars {
@@ -38,7 +48,8 @@ struct CgScalars {
 
 // CG scalars of a start whose r.(Minv r) = rz was reduced by the kernel that
 // wrote r and p (thresh = atol + rtol*sqrt(rz)); one thread.
-__device__ __forceinline__ void cg_start(CgScalars* sc, double rz, double atol, double rtol) {
+__device__ __forceinline__ void cg_start(CgScalars* sc, double rz, double atol, DevScalar rtol_s) {
+    const double rtol = rtol_s.get();
     sc->rz[0] = rz;
     sc->rz[1] = 0.0;
     sc->pq = 0.0;
@@ -55,7 +66,7 @@ __device__ __forceinline__ void cg_start(CgScalars* sc, double rz, double atol, 
 template <typename TV>
 static __global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
                                const TV* __restrict__ Minv, TV* __restrict__ r, TV* __restrict__ p,
-                               RedWorkspace ws, CgScalars* sc, double atol, double rtol) {
+                               RedWorkspace ws, CgScalars* sc, double atol, DevScalar rtol_s) {
     double acc[1] = {0.0};
     CSIPM_GRID_LOOP(i, n) {
         double rv = rhs[i];
@@ -69,7 +80,7 @@ static __global__ void cg_init_kernel(long long n, const double* __restrict__ rh
         const double rz = ws.out[0];
         sc->rz[0] = rz;
         sc->rz0 = rz;
-        sc->thresh = atol + rtol * sqrt(rz);
+        sc->thresh = atol + rtol_s.get() * sqrt(rz);
         sc->iters = 0;
         sc->breakdown = 0;
         sc->done = (sqrt(rz) <= sc->thresh) ? 1 : 0;
@@ -300,7 +311,7 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
                                const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
                                const TD* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
                                const TR* rp, TD* __restrict__ x0, float* cr, float* __restrict__ cp,
-                               const float* __restrict__ cm, CgScalars* csc, RedWorkspace ws, double crtol) {
+                               const float* __restrict__ cm, CgScalars* csc, RedWorkspace ws, DevScalar crtol) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
     double acc[1] = {0.0};
     CSIPM_GRID_LOOP(i, n) {
@@ -329,6 +340,96 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
         if (x0) x0[i] = dba[i];
     }
     if (cr && grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) cg_start(csc, ws.out[0], 0.0, crtol);
+}
+
+// ------------------------------------------------------------------ IPM control
+// Device control block of csipm_solve.  After every residual pass a
+// one-thread kernel (ipm_stop_kernel) turns the pass's reductions into mu,
+// the LASSO duality gap and the scaled KKT error, decides whether to stop,
+// and sets the Newton tolerance of the coming solves (forcing term); the
+// other kernels read mu, eta and the tolerances from here.  The host loop
+// reads the block once per iteration; a CUDA graph of whole iterations reads
+// nothing back until it ends.
+enum { IPM_RUNNING = 0, IPM_CONVERGED = 1, IPM_MAXITER = 2, IPM_NONFINITE = 3, IPM_ABORT = 4 };
+struct IpmCtl {
+    // set by the host at the start of a solve
+    double tol, rt_opt, forcing, rt_floor, rin_floor, z0sq, kkt_scale, lam, two_n;
+    int max_iter;
+    int k;              // iteration whose stop test ran last (-1 before the first)
+    // per iteration
+    double rt;          // relative tolerance of this iteration's Newton solves
+    double rin;         // max(rt, rin_floor): round 0 of a mixed-precision solve
+    double rt_next;     // the next iteration's (its residual pass starts the predictor CG)
+    double rin_next;
+    double mu, gap, kkt, F, obj, dual_inf, eta;
+    int status;         // IPM_*
+    int cg_iter;        // CG iterations run inside graph replays
+    int graph_iters;    // iterations completed inside graph replays
+    int abort_cg;       // graph replay stopped by a CG loop: 1 predictor, 2 corrector
+    int cg_done_last;   // pad
+    int pad;
+};
+
+// R: the residual pass's reductions (RR_*).  One thread.  With a conditional
+// handle (graph replays) the loop goes on while the status is IPM_RUNNING.
+static __global__ void ipm_stop_kernel(const double* __restrict__ R, IpmCtl* __restrict__ c, int in_graph,
+                                       cudaGraphConditionalHandle hnd) {
+    const int k = c->k + 1;
+    c->k = k;
+    const double mu = R[RR_SZ] / c->two_n;
+    const double usq = c->z0sq - 2.0 * R[RR_BB] + R[RR_BQB];
+    const double F = 0.5 * usq + c->lam * R[RR_L1];
+    const double th = R[RR_GINF] > 0.0 ? fmin(1.0, c->lam / R[RR_GINF]) : 1.0;
+    const double D = th * (c->z0sq - R[RR_BB]) - 0.5 * th * th * usq;
+    const double gap = (F - D) / fmax(fabs(F), 1e-300);
+    // scaled KKT error: the criterion that still applies when lambda = 0
+    // makes the LASSO dual bound degenerate
+    const double kkt = fmax(fmax(R[RR_RDINF], R[RR_RCINF]) / c->kkt_scale, R[RR_SZ] / fmax(1.0, fabs(F)));
+    c->mu = mu;
+    c->gap = gap;
+    c->kkt = kkt;
+    c->F = F;
+    c->obj = 0.5 * R[RR_BQB] - R[RR_BB] + c->lam * R[RR_SUMC];
+    c->dual_inf = R[RR_RDINF];
+    c->eta = fmax(0.99, 1.0 - mu);
+    int st = IPM_RUNNING;
+    if (!isfinite(mu) || !isfinite(gap)) st = IPM_NONFINITE;
+    else if (gap <= c->tol || kkt <= c->tol) st = IPM_CONVERGED;
+    else if (k >= c->max_iter) st = IPM_MAXITER;
+    c->status = st;
+    // this iteration solves at the tolerance its residual pass started with;
+    // the next one at the forcing term of this gap
+    c->rt = c->rt_next;
+    c->rin = c->rin_next;
+    const double rn = c->forcing > 0.0 ? fmin(c->rt_opt, fmax(c->rt_floor, c->forcing * gap)) : c->rt_opt;
+    c->rt_next = rn;
+    c->rin_next = fmax(rn, c->rin_floor);
+    if (in_graph) {
+        c->graph_iters += 1;
+        cudaGraphSetConditional(hnd, st == IPM_RUNNING ? 1u : 0u);
+    }
+}
+
+// Graph replays: opens a CG loop (a conditional while node) unless its start
+// already met the tolerance.  One thread.
+static __global__ void cg_arm_kernel(cudaGraphConditionalHandle hnd, const CgScalars* __restrict__ sc) {
+    cudaGraphSetConditional(hnd, sc->done ? 0u : 1u);
+}
+
+// Graph replays: after a CG loop, count its iterations and let the rest of
+// the iteration run only if it converged (a breakdown, or the loop's cap
+// below the solve's iteration cap, hands the iteration back to the host).
+static __global__ void ipm_cg_check_kernel(const CgScalars* __restrict__ sc, IpmCtl* __restrict__ c, int which,
+                                           int cap_is_limit, cudaGraphConditionalHandle if_hnd,
+                                           cudaGraphConditionalHandle loop_hnd) {
+    const bool ok = !sc->breakdown && (sc->done || cap_is_limit);
+    c->cg_iter += sc->iters;
+    if (!ok) {
+        c->status = IPM_ABORT;
+        c->abort_cg = which;
+        cudaGraphSetConditional(loop_hnd, 0u);
+    }
+    cudaGraphSetConditional(if_hnd, ok ? 1u : 0u);
 }
 
 // Step statistics of a direction: min ratios (primal, dual) and the sums for mu_aff.
@@ -391,18 +492,23 @@ ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, co
 }
 
 // Centring target after the predictor (Mehrotra): a = min(1, primal and dual
-// ratios), mu_aff = (s'z + a cross + a^2 dd)/(2n), sigma = (mu_aff/mu)^3;
+// ratios), mu_aff = (s'z + a cross + a^2 dd)/(2n), sigma = min(1, mu_aff/mu)^3;
 // q: the predictor's step statistics.  One thread.
-static __global__ void ipm_sigma_kernel(const double* __restrict__ q, double mu, double two_n, double* __restrict__ sigmu) {
+static __global__ void ipm_sigma_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+                                        double* __restrict__ sigmu) {
+    const double mu = c->mu, two_n = c->two_n;
     const double a = fmin(1.0, fmin(q[SS_MINP], q[SS_MIND]));
     const double mu_aff = (q[SS_SZ] + a * q[SS_CROSS] + a * a * q[SS_DD]) / two_n;
-    const double r = fmax(mu_aff, 0.0) / mu;
+    const double r = fmin(1.0, fmax(mu_aff, 0.0) / mu);   // sigma <= 1: the target never rises above mu
     *sigmu = r * r * r * mu;
 }
 
 // Step length after the corrector: min over primal and dual of
-// min(1, eta * ratio) (the same step for both).  One thread.
-static __global__ void ipm_alpha_kernel(const double* __restrict__ q, double eta, double* __restrict__ alpha) {
+// min(1, eta * ratio) (the same step for both), eta = max(0.99, 1 - mu) from
+// the control block.  One thread.
+static __global__ void ipm_alpha_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+                                        double* __restrict__ alpha) {
+    const double eta = c->eta;
     const double ap = fmin(1.0, eta * q[SS_MINP]);
     const double ad = fmin(1.0, eta * q[SS_MIND]);
     *alpha = fmin(ap, ad);
@@ -459,7 +565,7 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
                    const double* __restrict__ alpha_p, double* __restrict__ rd, double* __restrict__ Db,
                    double* __restrict__ Minv, TV* __restrict__ Db_lo, TV* __restrict__ Minv_lo, int precond,
                    double* __restrict__ rhs, RedWorkspace ws, TV* __restrict__ cr, TV* __restrict__ cp,
-                   CgScalars* csc, double crtol) {
+                   CgScalars* csc, DevScalar crtol) {
     double acc[RR_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const bool step = db != nullptr;
     const double sigmu = step ? *sigmu_p : 0.0;
@@ -591,6 +697,10 @@ struct EpiGrad {
 };
 
 static __global__ void fill_kernel(long long n, double v, double* __restrict__ y) {
+    CSIPM_GRID_LOOP(i, n) y[i] = v;
+}
+
+static __global__ void fill_f32_kernel(long long n, float v, float* __restrict__ y) {
     CSIPM_GRID_LOOP(i, n) y[i] = v;
 }
 

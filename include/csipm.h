@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define CSIPM_ABI_VERSION 1
+#define CSIPM_ABI_VERSION 2
 
 typedef enum {
     CSIPM_OK = 0,
@@ -89,14 +89,23 @@ typedef struct {
                                   "solver order" where the operator supports it (2D/3D), 1 the
                                   reference packing throughout.  Inputs and outputs of every entry
                                   point are in the reference packing either way. */
-    int cuda_graphs;           /* 1 (default): every CG loop of csipm_solve / csipm_admm runs as one
-                                  CUDA graph launch (a conditional while node over the iterations,
-                                  captured once per handle); 0: plain launches (same kernels, same
-                                  results) */
+    int cuda_graphs;           /* 1 (default): csipm_solve runs its iterations after the first as one
+                                  CUDA graph launch (a conditional while node over whole iterations,
+                                  the stop test on the device, nested while nodes for the CG loops)
+                                  when no Newton solve needs a host decision (FP64, or mixed with
+                                  ipm_cg_rtol >= 1e-4), else each CG loop of csipm_solve /
+                                  csipm_admm as one graph launch; graphs are captured once per
+                                  handle; 0: plain launches (same kernels, same results) */
     int autotune;              /* 1 (default): csipm_create times the candidate launch configurations
                                   of the FFT passes for this size (two-level vs Stockham kernels,
                                   lines / rows per CTA) once per process and keeps the fastest;
                                   0: the built-in heuristic */
+    double ipm_cg_forcing;     /* csipm_solve: forcing term of the inexact Newton solves.  Iteration k
+                                  solves to min(ipm_cg_rtol, max(1e-6, ipm_cg_forcing * gap[k-1]))
+                                  with gap[k-1] the previous iteration's relative duality gap, so
+                                  loose solves tighten as the method converges (fixed loose solves
+                                  stall once the gap is far below their accuracy); default 100,
+                                  0: every solve at ipm_cg_rtol */
 } csipm_options;
 
 /* Per-solve statistics (MadNLPExecutionStats analogue + the reference's timers,
@@ -118,9 +127,13 @@ typedef struct {
     /* the residual pass (the solve's largest kernel: pending step, residual,
      * barrier diagonals, predictor right-hand side), timed with CUDA events on
      * the solve's stream around each launch */
-    double resid_pass_ms;      /* device time of all its launches */
+    double resid_pass_ms;      /* device time of the launches the host ran (the first of a solve run
+                                  with cuda_graphs; every one without) */
     double resid_pass_bytes;   /* their algorithmic bytes (vectors read + written) */
-    int resid_pass_launches;   /* its launches (IPM iterations + 1) */
+    int resid_pass_launches;   /* the launches timed */
+    int graph_iters;           /* iterations run inside replays of the whole-iteration CUDA graph
+                                  (cuda_graphs = 1, FP64 or mixed with ipm_cg_rtol >= 1e-4): the
+                                  stop test runs on the device and the host waits once per solve */
 } csipm_stats;
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -253,16 +266,18 @@ CSIPM_API int csipm_get_timers(csipm_handle h, double* operator_ms, double* elem
  * memory limit, a serving process that pre-commits all HBM to resident
  * problems) and for loops that cannot afford cudaMalloc's implicit device
  * synchronisation.  It calls no cudaMalloc, cudaFree or allocating library
- * routine: its scratch (the half spectrum and the twiddle tables) lives in one
- * file-scope device array of 32 MiB that every GPU loading the library holds
- * until the process exits.  Problems whose half spectrum ((N1/2+1)*N2*N3
- * complex values) and twiddle tables need more than 32 MiB — above about 2.09
- * million complex values, e.g. 3D grids beyond 160^3 — are rejected with
- * CSIPM_ERR_UNSUPPORTED and a message.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
- * the array and each rewrites what it reads, so calls that overlap on the GPU
- * race: serialise them (one stream, or events).  Inputs and outputs are the
+ * routine and copies nothing from the host: its scratch (the half spectrum
+ * and the twiddle tables, which a small kernel writes on every call) lives in
+ * one file-scope device array of 32 MiB that every GPU loading the library
+ * holds until the process exits.  Problems whose half spectrum
+ * ((N1/2+1)*N2*N3 complex values) and twiddle tables need more than 32 MiB —
+ * above about 2.09 million complex values, e.g. 3D grids beyond 160^3; 1D
+ * lengths up to 2^20 fit — are rejected with CSIPM_ERR_UNSUPPORTED and a
+ * message.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array and each rewrites
+ * what it reads, so calls that overlap on the GPU race: serialise them (one
+ * stream, or events).  Inputs and outputs are the
  * caller's: x, y (N, device), keep_bits (device, or NULL for no missing
  * samples): one bit per sample, 1 = observed, column-major, LSB first, each
  * dim-1 row of N1 bits padded to a whole number of 32-bit words.  Runs on
@@ -329,13 +344,16 @@ typedef struct {
     int slots;                 /* concurrent solves; 0: 8 */
     size_t hbm_budget;         /* device bytes admitted requests may hold; 0: 80% of the free memory at create */
     int device;                /* CUDA device; -1: the current one */
+    int cuda_graphs;           /* 1: each request's solve runs its iterations as one graph launch
+                                  (captured per request); 0 (default): plain launches */
 } csipm_server_options;
 
 typedef struct {
     csipm_problem problem;     /* as for csipm_create, but z0 is a HOST pointer (N reals) */
     csipm_options options;     /* from csipm_default_options, then edited; `stream` and
                                   `cuda_graphs` are ignored (each request's handle lives for one
-                                  solve on its slot's stream; its CG loops run as plain launches) */
+                                  solve on its slot's stream; csipm_server_options.cuda_graphs
+                                  decides for all requests) */
     double* beta_out;          /* HOST, N reals, written before the result is posted (may be NULL) */
     uint64_t tag;              /* the caller's id, returned with the result */
 } csipm_request;
@@ -347,6 +365,7 @@ typedef struct {
     double queue_ms;           /* submission -> admission */
     double latency_ms;         /* submission -> result posted (beta_out written) */
     size_t footprint;          /* device bytes the request was admitted with */
+    char message[160];         /* the failure's message when status != 0 (truncated), else "" */
 } csipm_result;
 
 /* Device bytes a handle for this problem holds plus the server's staging of
@@ -354,7 +373,8 @@ typedef struct {
 CSIPM_API int csipm_footprint(int dim, const int* size, int precision, int64_t n_missing, size_t* bytes);
 CSIPM_API int csipm_server_create(const csipm_server_options* opt, csipm_server* out);
 /* Queues a copy of the request struct; the host buffers it points to must stay
- * valid until its result has been polled. */
+ * valid until its result has been polled.  A slot stages z0 and beta through
+ * pinned host buffers of its own, so its copies run asynchronously. */
 CSIPM_API int csipm_server_submit(csipm_server s, const csipm_request* r);
 /* Moves up to `max` finished results to `out` (*n of them), waiting up to
  * timeout_ms (-1: until one is ready or nothing is pending) when none is ready. */

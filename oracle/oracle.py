@@ -27,6 +27,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+import time
 
 import numpy as np
 import scipy.fft as sfft
@@ -339,6 +340,7 @@ class Operator:
         self.rdft = rdft
         self.workers = workers
         self.n_matvec = 0
+        self.t_matvec = 0.0        # seconds spent in AtA (the CPU baseline's unit costs)
 
     def A(self, beta):
         return M_perp_beta(beta, self.size, self.keep, self.rdft, self.workers)
@@ -348,4 +350,7 @@ class Operator:
 
     def AtA(self, x):
         self.n_matvec += 1
-        return M_perpt_M_perp_vec(x, self.size, self.keep, self.rdft, self.workers)
+        t0 = time.perf_counter()
+        y = M_perpt_M_perp_vec(x, self.size, self.keep, self.rdft, self.workers)
+        self.t_matvec += time.perf_counter() - t0
+        return y

@@ -87,11 +87,16 @@ def test_solver_order_matches_reference_order(cuda, kind, dims):
     assert abs(out["solver"].stats["lasso_obj"] - out["reference"].stats["lasso_obj"]) <= 1e-10 * abs(out["reference"].stats["lasso_obj"])
 
 
-@pytest.mark.parametrize("kind,dims,precision", [("3d", (32, 64, 24), "fp64"), ("2d", (96, 128), "mixed"),
-                                                 ("1d", (4096,), "fp64"), ("3d", (64, 64, 64), "mixed")])
-def test_cuda_graph_replay_changes_nothing(cuda, kind, dims, precision):
-    """Groups of CG iterations replayed from CUDA graphs run the same kernels
-    with the same arguments as plain launches: identical beta and counts."""
+@pytest.mark.parametrize("kind,dims,precision,rtol", [("3d", (32, 64, 24), "fp64", 1e-8), ("2d", (96, 128), "mixed", 1e-8),
+                                                      ("1d", (4096,), "fp64", 1e-8), ("3d", (64, 64, 64), "mixed", 1e-8),
+                                                      ("3d", (64, 64, 64), "fp64", 1e-2), ("3d", (48, 40, 36), "mixed", 1e-2),
+                                                      ("2d", (128, 96), "mixed", 1e-3), ("1d", (16384,), "fp64", 1e-2)])
+def test_cuda_graph_replay_changes_nothing(cuda, kind, dims, precision, rtol):
+    """Graph replays run the same kernels with the same arguments as plain
+    launches: identical beta and counts.  FP64 solves, and mixed ones with
+    FP32 directions (Newton rtol >= 1e-4), replay whole iterations (the stop
+    test on the device, one host wait per solve); the rest replay their CG
+    loops."""
     import csipm
     torch = cuda
     prob = _problem(kind, dims, seed=4)
@@ -99,13 +104,38 @@ def test_cuda_graph_replay_changes_nothing(cuda, kind, dims, precision):
     out = {}
     for graphs in (True, False):
         params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
-        nlp = csipm.FFTNLPModel(params, rdft=True, precision=precision, tol=1e-10, cuda_graphs=graphs)
+        nlp = csipm.FFTNLPModel(params, rdft=True, precision=precision, tol=1e-10, cuda_graphs=graphs,
+                                ipm_cg_rtol=rtol)
         res = csipm.ipm_solve(nlp)
         assert res.status == 0, res.stats
         out[graphs] = res
     assert torch.equal(out[True].beta, out[False].beta)
     for key in ("ipm_iter", "cg_iter", "matvecs"):
         assert out[True].stats[key] == out[False].stats[key]
+    whole = precision == "fp64" or rtol >= 1e-4
+    assert out[False].stats["graph_iters"] == 0
+    if whole:   # every iteration after the first ran inside the graph
+        assert out[True].stats["graph_iters"] == out[True].stats["ipm_iter"]
+    else:
+        assert out[True].stats["graph_iters"] == 0
+
+
+def test_graph_replay_stops_at_max_iter(cuda):
+    """The device stop test honours max_iter: a replayed solve capped at 3
+    iterations stops there, like the plain loop."""
+    import csipm
+    torch = cuda
+    prob = _problem("3d", (32, 32, 32), seed=2)
+    size = prob.size
+    got = {}
+    for graphs in (True, False):
+        params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
+        nlp = csipm.FFTNLPModel(params, rdft=True, tol=1e-10, max_iter=3, cuda_graphs=graphs, ipm_cg_rtol=1e-2)
+        res = csipm.ipm_solve(nlp)
+        assert res.status == -8, res.stats
+        got[graphs] = res
+    assert got[True].stats["ipm_iter"] == got[False].stats["ipm_iter"] == 3
+    assert torch.equal(got[True].beta, got[False].beta)
 
 
 @pytest.mark.parametrize("kind,dims", [("3d", (48, 40, 36)), ("2d", (100, 96)), ("3d", (32, 64, 24))])

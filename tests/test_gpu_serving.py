@@ -37,10 +37,13 @@ def _alone(torch, prob, precision, rtol):
     return res
 
 
-def test_results_same_alone_and_in_the_mix(cuda, problems):
+@pytest.mark.parametrize("graphs", [False, True])
+def test_results_same_alone_and_in_the_mix(cuda, problems, graphs):
+    """Served with plain launches or with each request's iterations as one
+    graph launch, every result equals the request solved alone."""
     from csipm.serving import Server
     torch = cuda
-    with Server(slots=4) as srv:
+    with Server(slots=4, cuda_graphs=graphs) as srv:
         for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
             srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=prec, tol=1e-10,
                        ipm_cg_rtol=rtol)
@@ -109,3 +112,22 @@ def test_footprint_bounds_the_handle(cuda, problems):
         fp = footprint(size, prec, prob.missing.size if prob.missing is not None else 0)
         nlp.op_fft.close()
         assert held <= fp <= 1.6 * held + (8 << 20), (size, held, fp)
+
+
+def test_failed_request_reports_its_message(cuda, problems):
+    """A request the library rejects comes back with its status and the
+    failure's message (the worker's error does not stay on its thread); the
+    requests around it still succeed."""
+    from csipm import _native
+    from csipm.serving import Server
+    good = problems[0]
+    n = int(np.prod(good.size))
+    with Server(slots=2) as srv:
+        srv.submit(good.size, good.z0, good.lam, good.missing, tag=0, precision="fp64", tol=1e-8)
+        srv.submit(good.size, good.z0, good.lam, np.array([0, n + 5], dtype=np.int64), tag=1, precision="fp64")
+        srv.submit(good.size, good.z0, good.lam, good.missing, tag=2, precision="fp64", tol=1e-8)
+        got = {r.tag: r for r in srv.drain()}
+    assert got[0].status == 0 and got[2].status == 0
+    assert got[0].message == ""
+    assert got[1].status == _native.CSIPM_ERR_INVALID
+    assert "out of range" in got[1].message
