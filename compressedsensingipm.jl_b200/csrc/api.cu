@@ -96,6 +96,20 @@ static __global__ void solver_order_kernel(Geom g, const double* __restrict__ in
     }
 }
 
+// Solver-order plane map: (re, im, kind, src) of the planes i = 0 and i = M1,
+// entry (p*N3 + k)*N2 + j, with re / im as solver-order tail indices.
+static __global__ void plane_map_kernel(Geom g, int4* __restrict__ pm) {
+    const int64_t per = (int64_t)g.n2 * g.n3;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < 2 * per;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(idx / per);
+        const int64_t r = idx - p * per;
+        const int k = (int)(r / g.n2), j = (int)(r % g.n2);
+        const MapEntry e = decode(g, p ? g.m1 : 0, j, k);
+        pm[idx] = make_int4((int)sol_tail(g, e.re), e.kind == KIND_VERT ? -1 : (int)sol_tail(g, e.im), e.kind, e.src);
+    }
+}
+
 cudaError_t to_solver_order(const Geom& g, const double* ref, double* sol, cudaStream_t st) {
     solver_order_kernel<true><<<ew_blocks(g.N / 2 + 1), EW_THREADS, 0, st>>>(g, ref, sol);
     return cudaGetLastError();
@@ -521,6 +535,24 @@ int profile_impl(csipm_handle h, FftOperator<T>& op, const T* x, T* D, T* q, int
 }
 
 
+// ------------------------------------------------------------------ IPM state
+// The vectors of csipm_solve / csipm_admm (and of csipm_profile_passes),
+// allocated on first use from the handle's stream-ordered pool; only the
+// missing ones are allocated.
+int ensure_ipm_buffers(csipm_handle h) {
+    const size_t n_ = (size_t)h->N;
+    double** f64[] = {&h->beta, &h->c, &h->s1, &h->s2, &h->z1, &h->z2, &h->rd, &h->Db, &h->Minv, &h->dba, &h->db,
+                      &h->cg_r, &h->cg_p, &h->cg_q};
+    for (double** q : f64)
+        if (!*q && !h->alloc(q, n_)) return fail(h, CSIPM_ERR_OOM, h->err);
+    if (h->opt.precision == CSIPM_MIXED) {
+        float** f32[] = {&h->f_Db, &h->f_Minv, &h->f_r, &h->f_p, &h->f_q, &h->f_x, &h->f_dba, &h->f_db};
+        for (float** q : f32)
+            if (!*q && !h->alloc(q, n_)) return fail(h, CSIPM_ERR_OOM, h->err);
+    }
+    return CSIPM_OK;
+}
+
 // ------------------------------------------------------------------ IPM iteration pieces
 // What csipm_solve's options make of an iteration.
 struct IpmMode {
@@ -678,8 +710,11 @@ bool build_ipm_graph(csipm_handle h, const IpmMode& md) {
     const bool pc = h->opt.preconditioner != 0;
     const double* Minv = pc ? h->Minv : nullptr;
     const float* Minv32 = pc ? h->f_Minv : nullptr;
+    // an FP32 round that is not done at its cap goes on to FP64 refinement on
+    // the host; an FP64 loop that reached the solve's own cap is accepted, as
+    // the plain loop accepts it
     const int cap = md.dir32 ? std::min(maxit, MIXED_ROUND_MAXIT) : std::min(maxit, CG_WHILE_CAP);
-    const int cap_is_limit = cap >= maxit ? 1 : 0;
+    const int cap_is_limit = (!md.dir32 && cap >= maxit) ? 1 : 0;
     const double* rt_dev = &h->ctl->rt;
     int kernels = 0;
     cudaStream_t ss[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -930,17 +965,12 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s2_cfg.grid.x * h->op64.s2_cfg.grid.y);
     if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s3_cfg.grid.x * h->op64.s3_cfg.grid.y);
     const size_t n_ = (size_t)h->N;
+    // the interior-point state is allocated by the first csipm_solve /
+    // csipm_admm (ensure_ipm_buffers): a handle used as an operator or a KKT
+    // plugin holds only the operator, A^T z0 and two scratch vectors
     if (!h->alloc(&h->partials, maxblocks * 8) || !h->alloc(&h->ticket, 1) || !h->alloc(&h->slots, SL_COUNT) ||
-        !h->alloc(&h->cgs, 1) || !h->alloc(&h->ctl, 1) || !h->alloc(&h->b, n_) || !h->alloc(&h->beta, n_) ||
-        !h->alloc(&h->c, n_) ||
-        !h->alloc(&h->s1, n_) || !h->alloc(&h->s2, n_) ||
-        !h->alloc(&h->z1, n_) || !h->alloc(&h->z2, n_) || !h->alloc(&h->Qb, n_) || !h->alloc(&h->rd, n_) ||
-        !h->alloc(&h->Db, n_) || !h->alloc(&h->Minv, n_) || !h->alloc(&h->rhs, n_) || !h->alloc(&h->dba, n_) ||
-        !h->alloc(&h->db, n_) || !h->alloc(&h->cg_r, n_) || !h->alloc(&h->cg_p, n_) || !h->alloc(&h->cg_q, n_))
-        return bail(CSIPM_ERR_OOM, h->err);
-    if (mixed && (!h->alloc(&h->f_Db, n_) || !h->alloc(&h->f_Minv, n_) || !h->alloc(&h->f_r, n_) ||
-                  !h->alloc(&h->f_p, n_) || !h->alloc(&h->f_q, n_) || !h->alloc(&h->f_x, n_) ||
-                  !h->alloc(&h->f_dba, n_) || !h->alloc(&h->f_db, n_)))
+        !h->alloc(&h->cgs, 1) || !h->alloc(&h->ctl, 1) || !h->alloc(&h->b, n_) || !h->alloc(&h->Qb, n_) ||
+        !h->alloc(&h->rhs, n_))
         return bail(CSIPM_ERR_OOM, h->err);
     static_assert(sizeof(double) * SL_COUNT == csipm_handle_s::HSLOT_BYTES, "slot block size");
     static_assert(sizeof(CgScalars) <= csipm_handle_s::HCGS_BYTES, "CG scalar block size");
@@ -961,38 +991,22 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         cudaError_t e0 = op_At(h->op64, prob->z0, st_b, h->stream);
         if (e0 != cudaSuccess) return bail(CSIPM_ERR_CUDA, std::string("A^T z0 failed: ") + cudaGetErrorString(e0));
     }
-    ew_launch(dot2_kernel, h->N, h->stream, h->N, prob->z0, prob->z0, nullptr, nullptr, h->ws(h->slots + SL_DOT));
+    // ||z0||^2 stays on the device (csipm_solve's stop test reads it there)
+    ew_launch(dot2_kernel, h->N, h->stream, h->N, prob->z0, prob->z0, nullptr, nullptr, h->ws(h->slots + SL_Z0SQ));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bail(CSIPM_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e));
-    if (cudaMemcpyAsync(h->hslots + SL_DOT, h->slots + SL_DOT, sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
-        cudaStreamSynchronize(h->stream) != cudaSuccess)
-        return bail(CSIPM_ERR_CUDA, "synchronisation failed after A^T z0");
-    h->z0sq = h->hslots[SL_DOT];
     if (h->opt.layout == 0 && solver_order_ok(h->op64) && (!mixed || solver_order_ok(h->op32))) {
         if (!h->alloc(&h->bs, n_)) return bail(CSIPM_ERR_OOM, h->err);
-        // plane map: the entries of the planes i = 0 and i = M1 in solver order
+        // plane map: the entries of the planes i = 0 and i = M1 in solver
+        // order, built on the device (no host loop, no copy)
         const Geom& g = h->g;
-        std::vector<int4> pm((size_t)2 * g.n2 * g.n3);
-        for (int p = 0; p < 2; ++p)
-            for (int k = 0; k < g.n3; ++k)
-                for (int j = 0; j < g.n2; ++j) {
-                    const MapEntry e = decode(g, p ? g.m1 : 0, j, k);
-                    int4 t;
-                    t.x = (int)sol_tail(g, e.re);
-                    t.y = e.kind == KIND_VERT ? -1 : (int)sol_tail(g, e.im);
-                    t.z = e.kind;
-                    t.w = e.src;
-                    pm[((size_t)p * g.n3 + k) * g.n2 + j] = t;
-                }
-        if (!h->alloc(&h->pmap, pm.size())) return bail(CSIPM_ERR_OOM, h->err);
-        if (cudaMemcpyAsync(h->pmap, pm.data(), sizeof(int4) * pm.size(), cudaMemcpyHostToDevice, h->stream) !=
-            cudaSuccess)
-            return bail(CSIPM_ERR_CUDA, "plane map upload failed");
+        const size_t np = (size_t)2 * g.n2 * g.n3;
+        if (!h->alloc(&h->pmap, np)) return bail(CSIPM_ERR_OOM, h->err);
+        plane_map_kernel<<<ew_blocks((long long)np), EW_THREADS, 0, h->stream>>>(g, h->pmap);
         h->op64.pmap = h->pmap;
         h->op32.pmap = h->pmap;
-        if (to_solver_order(h->g, h->b, h->bs, h->stream) != cudaSuccess ||
-            cudaStreamSynchronize(h->stream) != cudaSuccess)
-            return bail(CSIPM_ERR_CUDA, "solver-order copy of A^T z0 failed");
+        if (cudaGetLastError() != cudaSuccess || to_solver_order(h->g, h->b, h->bs, h->stream) != cudaSuccess)
+            return bail(CSIPM_ERR_CUDA, "solver-order set-up failed");
         h->sorder = true;
     }
     *out = h;
@@ -1053,6 +1067,10 @@ int csipm_apply_AtA(csipm_handle h, const double* x, double* y) {
 
 int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* stats) {
     if (!h || !beta_out) return fail(h, CSIPM_ERR_INVALID, "null argument");
+    {
+        const int r = ensure_ipm_buffers(h);
+        if (r) return r;
+    }
     const long long n = h->N;
     cudaStream_t st = h->stream;
     const double lam = h->lambda;
@@ -1093,7 +1111,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         c.forcing = o.ipm_cg_forcing;
         c.rt_floor = CG_FORCING_FLOOR;
         c.rin_floor = MIXED_INNER_RTOL;
-        c.z0sq = h->z0sq;
+        c.z0sq = 0.0;   // copied from the device slot below
         c.kkt_scale = std::max(1.0, h->hslots[SL_MAXB + 1]);
         c.lam = lam;
         c.two_n = 2.0 * (double)n;
@@ -1103,6 +1121,7 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
         c.rin_next = std::max(o.ipm_cg_rtol, MIXED_INNER_RTOL);
         c.status = IPM_RUNNING;
         CK(cudaMemcpyAsync(h->ctl, h->hctl, sizeof(IpmCtl), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(&h->ctl->z0sq, h->slots + SL_Z0SQ, sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     const double* rt_dev = &h->ctl->rt;
     const double* rin_dev = &h->ctl->rin;
@@ -1253,6 +1272,10 @@ int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* st
 
 int csipm_admm(csipm_handle h, double rho, int maxt, double tol, double* z_out, csipm_admm_stats* stats) {
     if (!h || !z_out) return fail(h, CSIPM_ERR_INVALID, "null argument");
+    {
+        const int r = ensure_ipm_buffers(h);
+        if (r) return r;
+    }
     if (!(rho > 0.0) || maxt < 0) return fail(h, CSIPM_ERR_INVALID, "rho must be > 0 and maxt >= 0");
     const long long n = h->N;
     cudaStream_t st = h->stream;
@@ -1340,6 +1363,14 @@ int csipm_profile_passes(csipm_handle h, const double* x, int reps, double* ms_o
     if (!h || !x || !ms_out || !bytes_out || !npass || reps < 1) return fail(h, CSIPM_ERR_INVALID, "bad argument");
     const char* names[8];
     int np = 0, r = 0;
+    // only the vectors of one CG product: D, q (and the FP32 copy of x)
+    if (h->opt.precision == CSIPM_MIXED) {
+        if ((!h->f_p && !h->alloc(&h->f_p, (size_t)h->N)) || (!h->f_Db && !h->alloc(&h->f_Db, (size_t)h->N)) ||
+            (!h->f_q && !h->alloc(&h->f_q, (size_t)h->N)))
+            return fail(h, CSIPM_ERR_OOM, h->err);
+    } else if ((!h->Db && !h->alloc(&h->Db, (size_t)h->N)) || (!h->cg_q && !h->alloc(&h->cg_q, (size_t)h->N))) {
+        return fail(h, CSIPM_ERR_OOM, h->err);
+    }
     if (h->opt.precision == CSIPM_MIXED) {
         // the FP32 passes of the CG product, on x rounded to FP32
         ew_launch(convert_kernel<double, float>, h->N, h->stream, h->N, x, h->f_p);

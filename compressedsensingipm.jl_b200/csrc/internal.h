@@ -94,7 +94,6 @@ struct csipm_handle_s {
     Geom g{};
     long long N = 0;
     double lambda = 0.0;
-    double z0sq = 0.0;
     FftOperator<double> op64;
     FftOperator<float> op32;        // mixed precision: the CG products
     std::string err;
@@ -214,7 +213,8 @@ inline int fail(csipm_handle h, int status, const std::string& msg) {
     } while (0)
 
 // slot indices in h->slots
-enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_SIGMU = 48, SL_ALPHA = 49, SL_COUNT = 64 };
+enum { SL_RED = 0, SL_MAXB = 16, SL_SS = 24, SL_DUMMY = 32, SL_DOT = 40, SL_SIGMU = 48, SL_ALPHA = 49, SL_Z0SQ = 50,
+       SL_COUNT = 64 };
 
 // ------------------------------------------------------------------ pass dispatch
 // Strided pass along `axis`: the two-level register kernel when the axis has

@@ -12,10 +12,18 @@
 //   dim-1 rows:   two-level row kernel (pair) or Stockham with 1..16 rows per CTA
 //
 // Results are cached per process, so every later handle of the same size
-// starts with the tuned configuration at no cost.
+// starts with the tuned configuration at no cost.  When the environment
+// variable CSIPM_TUNE_CACHE names a file, the cache persists across
+// processes: the file's choices are read at the first tuning, and every new
+// choice is appended to it as one JSON object per line,
+//   {"elem": 4, "dim": 3, "n": [320, 320, 320], "masked": 1,
+//    "s3_two": 1, "s3_tb": 0, "s2_tb": 0, "row_two": 1, "row_rb": 0}
 #pragma once
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
 
 #include "internal.h"
@@ -42,6 +50,52 @@ inline std::mutex& tune_mu() {
 inline std::map<TuneKey, TuneChoice>& tune_cache() {
     static std::map<TuneKey, TuneChoice> c;
     return c;
+}
+
+// CSIPM_TUNE_CACHE: "" when unset
+inline const std::string& tune_cache_path() {
+    static const std::string p = [] {
+        const char* e = std::getenv("CSIPM_TUNE_CACHE");
+        return std::string(e ? e : "");
+    }();
+    return p;
+}
+
+// Reads the persisted choices once (tune_mu held); lines that do not parse are skipped.
+inline void tune_cache_load() {
+    static bool loaded = false;
+    if (loaded) return;
+    loaded = true;
+    const std::string& path = tune_cache_path();
+    if (path.empty()) return;
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return;
+    char line[512];
+    while (std::fgets(line, sizeof(line), f)) {
+        int elem, dim, n1, n2, n3, masked;
+        TuneChoice c;
+        if (std::sscanf(line,
+                        " {\"elem\": %d, \"dim\": %d, \"n\": [%d, %d, %d], \"masked\": %d, \"s3_two\": %d, "
+                        "\"s3_tb\": %d, \"s2_tb\": %d, \"row_two\": %d, \"row_rb\": %d}",
+                        &elem, &dim, &n1, &n2, &n3, &masked, &c.s3_two, &c.s3_tb, &c.s2_tb, &c.row_two,
+                        &c.row_rb) == 11)
+            tune_cache()[TuneKey{elem, dim, n1, n2, n3, masked}] = c;
+    }
+    std::fclose(f);
+}
+
+// Appends one choice to the persisted cache (tune_mu held).
+inline void tune_cache_append(const TuneKey& k, const TuneChoice& c) {
+    const std::string& path = tune_cache_path();
+    if (path.empty()) return;
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return;
+    std::fprintf(f,
+                 "{\"elem\": %d, \"dim\": %d, \"n\": [%d, %d, %d], \"masked\": %d, \"s3_two\": %d, "
+                 "\"s3_tb\": %d, \"s2_tb\": %d, \"row_two\": %d, \"row_rb\": %d}\n",
+                 std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k), std::get<5>(k),
+                 c.s3_two, c.s3_tb, c.s2_tb, c.row_two, c.row_rb);
+    std::fclose(f);
 }
 
 // Stockham strided configuration with a forced number of lines per CTA
@@ -128,6 +182,7 @@ void autotune(FftOperator<T>& op, cudaStream_t st) {
     const TuneKey key{(int)sizeof(T), g.dim, g.n1, g.n2, g.n3, op.maskw ? 1 : 0};
     {
         std::lock_guard<std::mutex> lk(tune_mu());
+        tune_cache_load();
         auto it = tune_cache().find(key);
         if (it != tune_cache().end()) {
             apply_choice(op, it->second);
@@ -218,7 +273,7 @@ void autotune(FftOperator<T>& op, cudaStream_t st) {
     cudaEventDestroy(e1);
     {
         std::lock_guard<std::mutex> lk(tune_mu());
-        tune_cache()[key] = best;
+        if (tune_cache().emplace(key, best).second) tune_cache_append(key, best);
     }
     apply_choice(op, best);
 }

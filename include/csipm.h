@@ -99,7 +99,9 @@ typedef struct {
     int autotune;              /* 1 (default): csipm_create times the candidate launch configurations
                                   of the FFT passes for this size (two-level vs Stockham kernels,
                                   lines / rows per CTA) once per process and keeps the fastest;
-                                  0: the built-in heuristic */
+                                  with the environment variable CSIPM_TUNE_CACHE naming a file, the
+                                  choices persist there (one JSON object per line) and later
+                                  processes start from them; 0: the built-in heuristic */
     double ipm_cg_forcing;     /* csipm_solve: forcing term of the inexact Newton solves.  Iteration k
                                   solves to min(ipm_cg_rtol, max(1e-6, ipm_cg_forcing * gap[k-1]))
                                   with gap[k-1] the previous iteration's relative duality gap, so

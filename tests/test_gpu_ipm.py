@@ -154,3 +154,26 @@ def test_autotuned_and_heuristic_configs_agree(cuda, kind, dims):
         assert res.status == 0, res.stats
         out[tune] = res.beta.cpu().numpy()
     assert np.linalg.norm(out[True] - out[False]) <= 1e-7 * np.linalg.norm(out[False])
+
+
+def test_tune_cache_persists_across_processes(cuda, tmp_path):
+    """CSIPM_TUNE_CACHE names a file: the first process tunes a size and
+    appends its choice (one JSON object per line); a second process reads it
+    back and tunes nothing, so no second line appears."""
+    import json
+    import subprocess
+    import sys
+    from conftest import PKG
+    path = tmp_path / "tune.jsonl"
+    code = ("import sys; sys.path.insert(0, %r); import numpy as np, torch, csipm\n"
+            "size = (48, 40, 36)\n"
+            "z = torch.zeros(int(np.prod(size)), dtype=torch.float64, device='cuda')\n"
+            "op = csipm.FFTOperator(csipm.FFTParameters(3, size, z, 0.1, None), autotune=True)\n"
+            "op.close()\n") % PKG
+    env = dict(os.environ, CSIPM_TUNE_CACHE=str(path))
+    for _ in range(2):
+        subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
+    lines = path.read_text().splitlines()
+    assert len(lines) == 1
+    entry = json.loads(lines[0])
+    assert entry["n"] == [48, 40, 36] and entry["dim"] == 3 and entry["elem"] == 8

@@ -99,15 +99,20 @@ def test_requests_arriving_while_others_run(cuda, problems):
 
 
 def test_footprint_bounds_the_handle(cuda, problems):
-    """csipm_footprint is an upper bound of what a handle holds (+ the server's
-    z0/beta staging) and not far above it."""
+    """csipm_footprint is an upper bound of what a handle holds once it has
+    solved (+ the server's z0/beta staging) and not far above it; before its
+    first solve a handle holds only the operator, A^T z0 and two scratch
+    vectors (the interior-point state is allocated by the first solve)."""
     import csipm
     from csipm.serving import footprint
     torch = cuda
     for prob, (_, _, prec, rtol) in list(zip(problems, MIX))[:6]:
         size = prob.size
         params = csipm.FFTParameters(len(size), size, torch.tensor(prob.z0, device="cuda"), prob.lam, prob.missing)
-        nlp = csipm.FFTNLPModel(params, rdft=True, precision=prec)
+        nlp = csipm.FFTNLPModel(params, rdft=True, precision=prec, tol=1e-6)
+        before = nlp.op_fft.device_bytes()
+        csipm.ipm_solve(nlp)
+        assert nlp.op_fft.device_bytes() > before + 10 * 8 * int(np.prod(size))
         held = nlp.op_fft.device_bytes() + 16 * int(np.prod(size))
         fp = footprint(size, prec, prob.missing.size if prob.missing is not None else 0)
         nlp.op_fft.close()
