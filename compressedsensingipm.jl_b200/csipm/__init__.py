@@ -444,6 +444,23 @@ def CompressedSensingADMM(parameters: FFTParameters, fft_operator: "FFTOperator"
     return z
 
 
+def ipm_solve_batch(nlps, raise_on_error=False):
+    """Solves several FFTNLPModels together (csipm_solve_batch): every step is
+    one kernel launch for all of them.  The models must share the dimension
+    count, whether they have missing samples and (1D) whether N1/2 > 2048;
+    each keeps its own options.  Returns one SolveResult per model."""
+    torch = _torch()
+    k = len(nlps)
+    hs = (ctypes.c_void_p * k)(*[m.handle for m in nlps])
+    sols = [torch.empty(2 * m.nbeta, dtype=torch.float64, device=m.op_fft.z0.device) for m in nlps]
+    outs = (ctypes.c_void_p * k)(*[s.data_ptr() for s in sols])
+    st = (_native.Stats * k)()
+    status = lib().csipm_solve_batch(hs, k, outs, st)
+    if status not in (0, _native.CSIPM_ERR_IPM_MAXITER) or (raise_on_error and status != 0):
+        check(status)
+    return [SolveResult(sols[j], int(st[j].status), st[j].as_dict()) for j in range(k)]
+
+
 def ipm_solve(nlp: FFTNLPModel, raise_on_error=False):
     """ipm_solve!(solver) — src/CompressedSensingIPM.jl:31-36, on the device."""
     torch = _torch()

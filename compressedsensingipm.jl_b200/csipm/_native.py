@@ -37,6 +37,7 @@ EXPORTS = (
     "csipm_admm", "csipm_gondzio_obj", "csipm_gondzio_grad", "csipm_gondzio_cons", "csipm_gondzio_kkt_build",
     "csipm_gondzio_condensed_mul", "csipm_gondzio_precond_mul", "csipm_gondzio_kkt_mul", "csipm_gondzio_jtprod",
     "csipm_gondzio_kkt_solve", "csipm_footprint", "csipm_server_create", "csipm_server_submit", "csipm_server_poll", "csipm_server_destroy",
+    "csipm_solve_batch",
 )
 
 
@@ -159,6 +160,7 @@ def load(path: str | None = None):
         "csipm_jtprod": (I, [H, D, D]),
         "csipm_kkt_solve": (I, [H, D, D, ctypes.POINTER(I)]),
         "csipm_solve": (I, [H, D, D, ctypes.POINTER(Stats)]),
+        "csipm_solve_batch": (I, [ctypes.POINTER(H), I, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Stats)]),
         "csipm_get_timers": (I, [H, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.POINTER(dbl), I]),
         "csipm_profile_passes": (I, [H, D, I, ctypes.POINTER(dbl), ctypes.POINTER(dbl), ctypes.c_char_p, ctypes.POINTER(I)]),
         "csipm_apply_AtA_static": (I, [I, ctypes.POINTER(I), D, D, D, ctypes.c_void_p]),

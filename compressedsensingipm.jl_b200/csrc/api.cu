@@ -294,9 +294,7 @@ int schur_cg(csipm_handle h, const double* rhs, double* x, bool has_x0, double r
 // FP32 breakdown (p.q <= 0 from rounding on a nearly singular direction)
 // keeps the partial correction and finishes the solve with FP64 PCG.
 constexpr double MIXED_INNER_RTOL = 1e-6;
-// floor of csipm_solve's forcing term: no Newton solve is asked for more than
-// FP32 products reach, so FP64 and mixed precision take the same iterates
-constexpr double CG_FORCING_FLOOR = 1e-6;
+
 constexpr double MIXED_FP32_WARM_RTOL = 1e-4;
 constexpr int MIXED_ROUND_MAXIT = 100;
 

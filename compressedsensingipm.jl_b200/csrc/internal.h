@@ -392,6 +392,13 @@ cudaError_t to_reference_order(const Geom& g, const double* sol, double* ref, cu
 
 enum { RESID_NONE = 0, RESID_CG64 = 1, RESID_F32 = 2 };   // none / FP64 in cg_r / FP32 in f_r
 
+// floor of csipm_solve's forcing term: no Newton solve is asked for more than
+// FP32 products reach, so FP64 and mixed precision take the same iterates
+constexpr double CG_FORCING_FLOOR = 1e-6;
+
+// the interior-point vectors of csipm_solve / csipm_admm, allocated on first use
+int ensure_ipm_buffers(csipm_handle h);
+
 // Newton solves of the condensed system K x = rhs.  has_x0: x holds a start;
 // r0v (optional, with has_x0): rhs - K x0 is already known and no product
 // is spent on it.  xf (schur_mixed, optional): the start and the result are

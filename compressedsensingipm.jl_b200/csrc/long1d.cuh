@@ -25,7 +25,7 @@ namespace csipm {
 
 // ---------------------------------------------------------------- first pass
 template <typename T, typename TS>
-__global__ void __launch_bounds__(256) l1d_first_kernel(PassArgs<T> a, const TS* __restrict__ src,
+__device__ __forceinline__ void l1d_first_kernel_body(PassArgs<T> a, const TS* __restrict__ src,
                                                         const cplx_t<T>* __restrict__ twN, int P, int Q) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
@@ -62,11 +62,16 @@ __global__ void __launch_bounds__(256) l1d_first_kernel(PassArgs<T> a, const TS*
         }
     }
 }
+template <typename T, typename TS>
+__global__ void __launch_bounds__(256) l1d_first_kernel(PassArgs<T> a, const TS* __restrict__ src,
+                                                        const cplx_t<T>* __restrict__ twN, int P, int Q) {
+    l1d_first_kernel_body<T, TS>(a, src, twN, P, Q);
+}
 
 // ------------------------------------------------------------------ row pass
 // RB rows n2 per CTA, interleaved in shared memory as buf[n1*RB + b].
 template <typename T, int IN, int OUT, bool MASK>
-__global__ void __launch_bounds__(256) l1d_row_kernel(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, int P,
+__device__ __forceinline__ void l1d_row_kernel_body(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, int P,
                                                       int Q, int RB) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
@@ -129,11 +134,16 @@ __global__ void __launch_bounds__(256) l1d_row_kernel(PassArgs<T> a, const cplx_
         }
     }
 }
+template <typename T, int IN, int OUT, bool MASK>
+__global__ void __launch_bounds__(256) l1d_row_kernel(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, int P,
+                                                      int Q, int RB) {
+    l1d_row_kernel_body<T, IN, OUT, MASK>(a, twN, P, Q, RB);
+}
 
 // ------------------------------------------------------------------ post pass
 // X[k] from Z[k], Z[M-k] (k = 0 also gives X[M]) and the scatter to beta.
 template <typename T, class Epi>
-__global__ void __launch_bounds__(256) l1d_post_kernel(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, Epi epi) {
+__device__ __forceinline__ void l1d_post_kernel_body(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, Epi epi) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     const int M = a.g.m1;
@@ -154,6 +164,10 @@ __global__ void __launch_bounds__(256) l1d_post_kernel(PassArgs<T> a, const cplx
         }
     }
     ep.finish();
+}
+template <typename T, class Epi>
+__global__ void __launch_bounds__(256) l1d_post_kernel(PassArgs<T> a, const cplx_t<T>* __restrict__ twN, Epi epi) {
+    l1d_post_kernel_body<T, Epi>(a, twN, epi);
 }
 
 }  // namespace csipm

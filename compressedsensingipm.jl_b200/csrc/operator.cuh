@@ -228,7 +228,7 @@ constexpr int SCATTER_UNROLL = 4;
 // Shared memory: two load buffers (the next tile streams in by cp.async while
 // the current one is transformed) and one work buffer for the ping-pong stages.
 template <typename T, int TB, bool INV, int IN, int OUT, typename TS, class Epi>
-__global__ void __launch_bounds__(256) strided_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+__device__ __forceinline__ void strided_pass_kernel_body(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -315,6 +315,10 @@ __global__ void __launch_bounds__(256) strided_pass_kernel(PassArgs<T> a, const 
     }
     if (OUT == OUT_SCATTER) ep.finish();
 }
+template <typename T, int TB, bool INV, int IN, int OUT, typename TS, class Epi>
+__global__ void __launch_bounds__(256) strided_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    strided_pass_kernel_body<T, TB, INV, IN, OUT, TS, Epi>(a, src, epi);
+}
 
 // ---------------------------------------------------------------- row pass
 // Z[k] = (X[k] + conj X[M-k]) + i conj(W^k) (X[k] - conj X[M-k])   (C2R pre-processing)
@@ -334,7 +338,7 @@ __device__ __forceinline__ C r2c_post(C za, C zb, C w) {
 // (rows = (j, k) pairs), each row M+1 half-spectrum values, interleaved in
 // shared memory as buf[n*TBP + b].
 template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
-__global__ void __launch_bounds__(256) row_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+__device__ __forceinline__ void row_pass_kernel_body(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -463,6 +467,10 @@ __global__ void __launch_bounds__(256) row_pass_kernel(PassArgs<T> a, const TS* 
         __syncthreads();
     }
     if (OUT == OUT_SCATTER) ep.finish();
+}
+template <typename T, int IN, int OUT, bool MASK, typename TS, class Epi>
+__global__ void __launch_bounds__(256) row_pass_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
+    row_pass_kernel_body<T, IN, OUT, MASK, TS, Epi>(a, src, epi);
 }
 
 // In-place row pass for rows too long to double-buffer (1D with large N):

@@ -16,6 +16,8 @@ struct RedWorkspace {
     double* partials;        // [max_blocks * NV]
     unsigned int* ticket;    // one counter, zero between launches
     double* out;             // [NV] final values
+    int xonly = 0;           // 1: the blocks of one blockIdx.y / z reduce on their own (batched launches,
+                             // one instance per blockIdx.y, each with its own workspace)
 };
 
 __device__ __forceinline__ double red_op(double a, double b, int comp, unsigned maxmask, unsigned minmask) {
@@ -62,8 +64,8 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], unsigned maxmask, 
 template <int NV>
 __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const RedWorkspace& ws, unsigned maxmask, unsigned minmask) {
     block_reduce<NV>(v, maxmask, minmask);
-    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned nblocks = ws.xonly ? gridDim.x : gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = ws.xonly ? blockIdx.x : blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     __shared__ bool last;
     if (threadIdx.x == 0) {
 #pragma unroll

@@ -64,7 +64,7 @@ __device__ __forceinline__ void cg_start(CgScalars* sc, double rz, double atol, 
 // r = rhs - q (q = (Q + D) x0 computed by the operator), or r = rhs when x0 == 0;
 // z = Minv r ; p = z ; rz = r.z ; thresh = atol + rtol*sqrt(rz)
 template <typename TV>
-static __global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
+__device__ __forceinline__ void cg_init_kernel_body(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
                                const TV* __restrict__ Minv, TV* __restrict__ r, TV* __restrict__ p,
                                RedWorkspace ws, CgScalars* sc, double atol, DevScalar rtol_s) {
     double acc[1] = {0.0};
@@ -87,10 +87,16 @@ static __global__ void cg_init_kernel(long long n, const double* __restrict__ rh
         if (!isfinite(rz)) { sc->done = 1; sc->breakdown = 1; }
     }
 }
+template <typename TV>
+static __global__ void cg_init_kernel(long long n, const double* __restrict__ rhs, const TV* __restrict__ q, int has_x0,
+                               const TV* __restrict__ Minv, TV* __restrict__ r, TV* __restrict__ p,
+                               RedWorkspace ws, CgScalars* sc, double atol, DevScalar rtol_s) {
+    cg_init_kernel_body<TV>(n, rhs, q, has_x0, Minv, r, p, ws, sc, atol, rtol_s);
+}
 
 // alpha = rz/pq ; x += alpha p ; r -= alpha q ; rz' = r.(Minv r)
 template <typename TV, typename TX>
-static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
+__device__ __forceinline__ void cg_update_kernel_body(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
                                  const TV* __restrict__ q, const TV* __restrict__ Minv, RedWorkspace ws, CgScalars* sc) {
     if (sc->done) return;
     const double pq = sc->pq;
@@ -129,10 +135,15 @@ static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x,
         else if (sqrt(rzn) <= sc->thresh) sc->done = 1;
     }
 }
+template <typename TV, typename TX>
+static __global__ void cg_update_kernel(long long n, int it, TX* __restrict__ x, TV* __restrict__ r, const TV* __restrict__ p,
+                                 const TV* __restrict__ q, const TV* __restrict__ Minv, RedWorkspace ws, CgScalars* sc) {
+    cg_update_kernel_body<TV, TX>(n, it, x, r, p, q, Minv, ws, sc);
+}
 
 // p = Minv r + (rz'/rz) p
 template <typename TV>
-static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
+__device__ __forceinline__ void cg_pupdate_kernel_body(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
                                   const CgScalars* sc) {
     if (sc->done) return;
     const double b = sc->rz[(it + 1) & 1] / sc->rz[it & 1];
@@ -146,6 +157,11 @@ static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restri
         p[j] = (TV)(mj * rj + b * pj);
     }
     if (i < n) p[i] = (TV)((Minv ? (double)Minv[i] : 1.0) * (double)r[i] + b * (double)p[i]);
+}
+template <typename TV>
+static __global__ void cg_pupdate_kernel(long long n, int it, const TV* __restrict__ r, const TV* __restrict__ Minv, TV* __restrict__ p,
+                                  const CgScalars* sc) {
+    cg_pupdate_kernel_body<TV>(n, it, r, Minv, p, sc);
 }
 
 // Mixed precision: r = rhs - q in FP64 with r.(Minv r) (the refinement residual)
@@ -171,7 +187,7 @@ enum { RR_SZ = 0, RR_BB, RR_BQB, RR_L1, RR_GINF, RR_RDINF, RR_RCINF, RR_SUMC, RR
 constexpr unsigned RR_MAXMASK = (1u << RR_GINF) | (1u << RR_RDINF) | (1u << RR_RCINF);
 
 // beta = soft(b, lambda); reduce max|beta| and max|b|
-static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
+__device__ __forceinline__ void ipm_init1_kernel_body(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
                                  RedWorkspace ws) {
     double acc[2] = {0.0, 0.0};
     CSIPM_GRID_LOOP(i, n) {
@@ -184,6 +200,10 @@ static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ 
     }
     grid_reduce<2>(acc, ws, 3u, 0u);
 }
+static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ b, double lam, double* __restrict__ beta,
+                                 RedWorkspace ws) {
+    ipm_init1_kernel_body(n, b, lam, beta, ws);
+}
 
 // Dual start from the clipped gradient with lz = max(lambda, 1e-3 |b|_inf, 1e-12)
 // (the floor keeps lambda = 0 interior); c = |beta| + mu0/min(z1,z2),
@@ -191,7 +211,7 @@ static __global__ void ipm_init1_kernel(long long n, const double* __restrict__ 
 // The slacks s1 = c + beta, s2 = c - beta are the stored variables from here
 // on (MadNLP's slack formulation): recomputing them from c and beta would
 // cancel catastrophically once a bound is nearly active.
-static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+__device__ __forceinline__ void ipm_init2_kernel_body(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                                  const double* __restrict__ beta, const double* __restrict__ mx,
                                  double* __restrict__ s1, double* __restrict__ s2, double* __restrict__ z1,
                                  double* __restrict__ z2) {
@@ -208,6 +228,12 @@ static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ 
         s1[i] = ce + be;
         s2[i] = ce - be;
     }
+}
+static __global__ void ipm_init2_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+                                 const double* __restrict__ beta, const double* __restrict__ mx,
+                                 double* __restrict__ s1, double* __restrict__ s2, double* __restrict__ z1,
+                                 double* __restrict__ z2) {
+    ipm_init2_kernel_body(n, b, Qb, lam, beta, mx, s1, s2, z1, z2);
 }
 
 // Per-element quantities shared by every direction of one iteration:
@@ -307,7 +333,7 @@ __device__ __forceinline__ ElemDir elem_affine(const ElemPre& e, double lam, dou
 // null without one), r.(Minv r) reduced and the CG scalars set.  rp may be
 // the same vector as cr (read, then overwritten, by the same thread).
 template <typename TR, typename TD>
-static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+__device__ __forceinline__ void ipm_rhs_kernel_body(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                                const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
                                const TD* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
                                const TR* rp, TD* __restrict__ x0, float* cr, float* __restrict__ cp,
@@ -341,6 +367,14 @@ static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __r
     }
     if (cr && grid_reduce<1>(acc, ws, 0u, 0u) && threadIdx.x == 0) cg_start(csc, ws.out[0], 0.0, crtol);
 }
+template <typename TR, typename TD>
+static __global__ void ipm_rhs_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+                               const double* __restrict__ z1, const double* __restrict__ z2, double* rd,
+                               const TD* __restrict__ dba, const double* __restrict__ sigmu_p, double* rhs,
+                               const TR* rp, TD* __restrict__ x0, float* cr, float* __restrict__ cp,
+                               const float* __restrict__ cm, CgScalars* csc, RedWorkspace ws, DevScalar crtol) {
+    ipm_rhs_kernel_body<TR, TD>(n, lam, s1v, s2v, z1, z2, rd, dba, sigmu_p, rhs, rp, x0, cr, cp, cm, csc, ws, crtol);
+}
 
 // ------------------------------------------------------------------ IPM control
 // Device control block of csipm_solve.  After every residual pass a
@@ -372,7 +406,7 @@ struct IpmCtl {
 
 // R: the residual pass's reductions (RR_*).  One thread.  With a conditional
 // handle (graph replays) the loop goes on while the status is IPM_RUNNING.
-static __global__ void ipm_stop_kernel(const double* __restrict__ R, IpmCtl* __restrict__ c, int in_graph,
+__device__ __forceinline__ void ipm_stop_kernel_body(const double* __restrict__ R, IpmCtl* __restrict__ c, int in_graph,
                                        cudaGraphConditionalHandle hnd) {
     const int k = c->k + 1;
     c->k = k;
@@ -408,6 +442,10 @@ static __global__ void ipm_stop_kernel(const double* __restrict__ R, IpmCtl* __r
         c->graph_iters += 1;
         cudaGraphSetConditional(hnd, st == IPM_RUNNING ? 1u : 0u);
     }
+}
+static __global__ void ipm_stop_kernel(const double* __restrict__ R, IpmCtl* __restrict__ c, int in_graph,
+                                       cudaGraphConditionalHandle hnd) {
+    ipm_stop_kernel_body(R, c, in_graph, hnd);
 }
 
 // Graph replays: opens a CG loop (a conditional while node) unless its start
@@ -448,8 +486,7 @@ struct MinRatio {
 
 // TD: type the Newton directions are stored in (FP32 in loose mixed precision)
 template <typename TD>
-static __global__ void __launch_bounds__(EW_THREADS, 3)
-ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+__device__ __forceinline__ void ipm_stepstats_kernel_body(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
                      const double* __restrict__ z1, const double* __restrict__ z2, const TD* __restrict__ dba,
                      const double* __restrict__ sigmu_p, const TD* __restrict__ db, RedWorkspace ws) {
     const double sigmu = sigmu_p ? *sigmu_p : 0.0;
@@ -490,11 +527,18 @@ ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, co
     acc[SS_MIND] = md.value();
     grid_reduce<SS_N>(acc, ws, 0u, SS_MINMASK);
 }
+template <typename TD>
+static __global__ void __launch_bounds__(EW_THREADS, 3)
+ipm_stepstats_kernel(long long n, double lam, const double* __restrict__ s1v, const double* __restrict__ s2v,
+                     const double* __restrict__ z1, const double* __restrict__ z2, const TD* __restrict__ dba,
+                     const double* __restrict__ sigmu_p, const TD* __restrict__ db, RedWorkspace ws) {
+    ipm_stepstats_kernel_body<TD>(n, lam, s1v, s2v, z1, z2, dba, sigmu_p, db, ws);
+}
 
 // Centring target after the predictor (Mehrotra): a = min(1, primal and dual
 // ratios), mu_aff = (s'z + a cross + a^2 dd)/(2n), sigma = min(1, mu_aff/mu)^3;
 // q: the predictor's step statistics.  One thread.
-static __global__ void ipm_sigma_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+__device__ __forceinline__ void ipm_sigma_kernel_body(const double* __restrict__ q, const IpmCtl* __restrict__ c,
                                         double* __restrict__ sigmu) {
     const double mu = c->mu, two_n = c->two_n;
     const double a = fmin(1.0, fmin(q[SS_MINP], q[SS_MIND]));
@@ -502,16 +546,24 @@ static __global__ void ipm_sigma_kernel(const double* __restrict__ q, const IpmC
     const double r = fmin(1.0, fmax(mu_aff, 0.0) / mu);   // sigma <= 1: the target never rises above mu
     *sigmu = r * r * r * mu;
 }
+static __global__ void ipm_sigma_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+                                        double* __restrict__ sigmu) {
+    ipm_sigma_kernel_body(q, c, sigmu);
+}
 
 // Step length after the corrector: min over primal and dual of
 // min(1, eta * ratio) (the same step for both), eta = max(0.99, 1 - mu) from
 // the control block.  One thread.
-static __global__ void ipm_alpha_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+__device__ __forceinline__ void ipm_alpha_kernel_body(const double* __restrict__ q, const IpmCtl* __restrict__ c,
                                         double* __restrict__ alpha) {
     const double eta = c->eta;
     const double ap = fmin(1.0, eta * q[SS_MINP]);
     const double ad = fmin(1.0, eta * q[SS_MIND]);
     *alpha = fmin(ap, ad);
+}
+static __global__ void ipm_alpha_kernel(const double* __restrict__ q, const IpmCtl* __restrict__ c,
+                                        double* __restrict__ alpha) {
+    ipm_alpha_kernel_body(q, c, alpha);
 }
 
 // ------------------------------------------------------------------ ADMM (src/admm.jl)
@@ -557,8 +609,7 @@ static __global__ void admm_update_kernel(long long n, const double* __restrict_
 // precision), and the predictor right-hand side (h1 = -z1, h2 = -z2,
 // fc = -lambda).
 template <typename TV, typename TD>
-static __global__ void __launch_bounds__(EW_THREADS, 3)
-ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+__device__ __forceinline__ void ipm_resdiag_kernel_body(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
                    const double* __restrict__ beta, double* __restrict__ s1v, double* __restrict__ s2v,
                    double* __restrict__ z1, double* __restrict__ z2, const TD* __restrict__ dba,
                    const TD* __restrict__ db, const double* __restrict__ sigmu_p,
@@ -630,6 +681,18 @@ ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __re
              b[i]);
     if (grid_reduce<RR_N>(acc, ws, RR_MAXMASK, 0u) && csc && threadIdx.x == 0) cg_start(csc, ws.out[RR_RZ], 0.0, crtol);
 }
+template <typename TV, typename TD>
+static __global__ void __launch_bounds__(EW_THREADS, 3)
+ipm_resdiag_kernel(long long n, const double* __restrict__ b, const double* __restrict__ Qb, double lam,
+                   const double* __restrict__ beta, double* __restrict__ s1v, double* __restrict__ s2v,
+                   double* __restrict__ z1, double* __restrict__ z2, const TD* __restrict__ dba,
+                   const TD* __restrict__ db, const double* __restrict__ sigmu_p,
+                   const double* __restrict__ alpha_p, double* __restrict__ rd, double* __restrict__ Db,
+                   double* __restrict__ Minv, TV* __restrict__ Db_lo, TV* __restrict__ Minv_lo, int precond,
+                   double* __restrict__ rhs, RedWorkspace ws, TV* __restrict__ cr, TV* __restrict__ cp,
+                   CgScalars* csc, DevScalar crtol) {
+    ipm_resdiag_kernel_body<TV, TD>(n, b, Qb, lam, beta, s1v, s2v, z1, z2, dba, db, sigmu_p, alpha_p, rd, Db, Minv, Db_lo, Minv_lo, precond, rhs, ws, cr, cp, csc, crtol);
+}
 
 // FP64 barrier diagonals alone (mixed precision at loose Newton tolerances
 // skips them in the residual pass; the first FP64 product or FP64 fallback
@@ -647,16 +710,25 @@ static __global__ void ipm_diag64_kernel(long long n, const double* __restrict__
 // beta += alpha db (the slacks and multipliers take their step in the next
 // residual pass)
 template <typename TD>
-static __global__ void ipm_beta_step_kernel(long long n, double* __restrict__ beta, const TD* __restrict__ db,
+__device__ __forceinline__ void ipm_beta_step_kernel_body(long long n, double* __restrict__ beta, const TD* __restrict__ db,
                                             const double* __restrict__ alpha_p) {
     const double alpha = *alpha_p;
     CSIPM_GRID_LOOP(i, n) beta[i] += alpha * (double)db[i];
 }
+template <typename TD>
+static __global__ void ipm_beta_step_kernel(long long n, double* __restrict__ beta, const TD* __restrict__ db,
+                                            const double* __restrict__ alpha_p) {
+    ipm_beta_step_kernel_body<TD>(n, beta, db, alpha_p);
+}
 
 // c = (s1 + s2)/2
-static __global__ void half_sum_kernel(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
+__device__ __forceinline__ void half_sum_kernel_body(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
                                        double* __restrict__ c) {
     CSIPM_GRID_LOOP(i, n) c[i] = 0.5 * (s1[i] + s2[i]);
+}
+static __global__ void half_sum_kernel(long long n, const double* __restrict__ s1, const double* __restrict__ s2,
+                                       double* __restrict__ c) {
+    half_sum_kernel_body(n, s1, s2, c);
 }
 
 // ------------------------------------------------------------------ utilities

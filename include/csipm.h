@@ -252,6 +252,24 @@ CSIPM_API int csipm_kkt_solve(csipm_handle h, double* w, const double* pr_diag, 
  * the solution; stats may be NULL. */
 CSIPM_API int csipm_solve(csipm_handle h, double* beta_out, double* c_out, csipm_stats* stats);
 
+/* Batched solves: advances `count` handles' interior-point solves together,
+ * every step one kernel launch for all of them — the FFT passes are
+ * persistent Stockham kernels over an instance table (per instance its
+ * sizes, run-time plans, vector offsets, reduction workspace and control
+ * block) and every element kernel runs all instances at once (gridDim.y =
+ * instance).  Any sizes mix; the handles must share the dimension count,
+ * whether they have missing samples, and for 1D whether the rows take the
+ * long-row passes (N1/2 > 2048).  Each instance solves with its own options
+ * (tol, max_iter, ipm_cg_rtol, ipm_cg_forcing, preconditioner) by
+ * csipm_solve's FP64 method in the reference packing: its iterates equal
+ * csipm_solve's up to the order of floating-point sums.  Runs on hs[0]'s
+ * stream (the other handles' streams are joined first).  beta_out[k] (device,
+ * N_k values) and stats[k] (may be NULL) receive instance k's result; returns
+ * CSIPM_OK when every instance converged, else the first failure (each
+ * instance's status is in its stats).  No counterpart in the reference, which
+ * solves one recovery per call (src/CompressedSensingIPM.jl:31-36). */
+CSIPM_API int csipm_solve_batch(csipm_handle* hs, int count, double* const* beta_out, csipm_stats* stats);
+
 /* ---------------------------------------------------------------- timers */
 
 /* Device time (ms, CUDA events) accumulated by the handle in the three buckets
