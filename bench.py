@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="requests of the serving stream measured beside the headline solve (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
+    ap.add_argument("--serve-batch", type=int, default=32,
+                    help="requests of one batch class a slot solves together in the batched closed run (<= 1: skip)")
+    ap.add_argument("--serve-batch-slots", type=int, default=8, help="slots of the batched closed run")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving leg and print its JSON object (slot-count experiments)")
     ap.add_argument("--no-graphs", action="store_true",
@@ -675,12 +678,12 @@ def run_serving(args, n_req, slots, rank):
     seq_plain_rate, seq_plain_failed, seq_plain_share = sequential(dict(opts, cuda_graphs=False))
     seq_rate = max(seq_graph_rate, seq_plain_rate)
 
-    def serve(rate, graphs):
+    def serve(rate, graphs, batch=1, nslots=slots):
         rng = np.random.default_rng(7)
         gaps = rng.exponential(1.0 / rate, size=n_req) if rate else np.zeros(n_req)
         arrivals = np.cumsum(gaps) - gaps[0]
         res = []
-        with Server(slots=slots, cuda_graphs=graphs) as srv:
+        with Server(slots=nslots, cuda_graphs=graphs, batch=batch) as srv:
             t_start = time.perf_counter()
             for k, r in enumerate(reqs):
                 while True:
@@ -699,20 +702,30 @@ def run_serving(args, n_req, slots, rank):
         return {"solves_per_s": round(n_req / (t_end - t_start), 2),
                 "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
                 "failed": int(sum(x.status != 0 for x in res)),
+                "failures": sorted({x.message for x in res if x.status != 0})[:3],
+                "mean_group": round(float(np.mean([x.group for x in res])), 2),
                 "slot_time_share": {k: round(v / tot, 3) for k, v in busy.items()}}
 
-    # untimed: the first slots' worth of requests through the server (device
-    # memory pool and per-size kernel set-up warm, as in a running service)
-    with Server(slots=slots) as srv:
-        for k, r in enumerate(reqs[:slots]):
-            srv.submit(r["size"], r["z0"], r["lam"], r["missing"], tag=k, precision=r["precision"], **opts)
-        srv.drain()
+    # untimed: the first slots' worth of requests through the server, one at
+    # a time and batched (device memory pool and kernel set-up warm, as in a
+    # running service)
+    batch = int(getattr(args, "serve_batch", 1))
+    bslots = int(getattr(args, "serve_batch_slots", slots))
+    for warm_batch, warm_slots in (((1, slots), (batch, bslots)) if batch > 1 else ((1, slots),)):
+        with Server(slots=warm_slots, batch=warm_batch) as srv:
+            for k, r in enumerate(reqs[:max(warm_slots, 4 * warm_batch)]):
+                srv.submit(r["size"], r["z0"], r["lam"], r["missing"], tag=k, precision=r["precision"], **opts)
+            srv.drain()
     closed_plain = serve(0.0, False)
     closed_graphs = serve(0.0, True)
-    graphs = closed_graphs["solves_per_s"] > closed_plain["solves_per_s"]
-    closed = closed_graphs if graphs else closed_plain
+    closed_batched = serve(0.0, False, batch, bslots) if batch > 1 else None
+    # the fastest closed mode sets the Poisson run's mode and offered rate
+    modes = [(closed_plain, False, 1, slots), (closed_graphs, True, 1, slots)]
+    if closed_batched:
+        modes.append((closed_batched, False, batch, bslots))
+    closed, graphs, pbatch, pslots = max(modes, key=lambda m: m[0]["solves_per_s"])
     offered = 0.8 * closed["solves_per_s"]
-    poisson = serve(offered, graphs)
+    poisson = serve(offered, graphs, pbatch, pslots)
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("1d", "2d", "3d")}
     return {
         "requests": n_req, "slots": slots, "mix": kinds,
@@ -725,10 +738,15 @@ def run_serving(args, n_req, slots, rank):
                                      "faster of plain launches and the per-request iteration graph",
                              "graph_launches": {"solves_per_s": round(seq_graph_rate, 2), "time_share": seq_graph_share},
                              "plain_launches": {"solves_per_s": round(seq_plain_rate, 2), "time_share": seq_plain_share}},
-        "batched_closed": dict(closed, cuda_graphs=graphs),
+        "batched_closed": dict(closed, cuda_graphs=graphs, batch=pbatch, slots=pslots),
         "batched_closed_plain_launches": closed_plain,
         "batched_closed_graph_launches": closed_graphs,
-        "batched_poisson": dict(poisson, offered_per_s=round(offered, 2), cuda_graphs=graphs),
+        "batched_closed_solve_batch": (dict(closed_batched, batch=batch, slots=bslots,
+                                            what="each slot solves up to `batch` admitted requests of one batch "
+                                                 "class together (csipm_solve_batch, FP64)")
+                                       if closed_batched else None),
+        "batched_poisson": dict(poisson, offered_per_s=round(offered, 2), cuda_graphs=graphs, batch=pbatch,
+                                slots=pslots),
         "speedup_vs_sequential": round(closed["solves_per_s"] / seq_rate, 2),
     }
 

@@ -108,7 +108,7 @@ class AdmmStats(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("device", ctypes.c_int),
-                ("cuda_graphs", ctypes.c_int)]
+                ("cuda_graphs", ctypes.c_int), ("batch", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):
@@ -117,7 +117,8 @@ class Request(ctypes.Structure):
 
 class Result(ctypes.Structure):
     _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int), ("stats", Stats), ("queue_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_size_t), ("message", ctypes.c_char * 160)]
+                ("latency_ms", ctypes.c_double), ("footprint", ctypes.c_size_t), ("message", ctypes.c_char * 160),
+                ("group", ctypes.c_int)]
 
 
 

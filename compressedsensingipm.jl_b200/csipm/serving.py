@@ -43,15 +43,17 @@ class ServeResult:
     footprint: int
     beta: np.ndarray = field(repr=False, default=None)
     message: str = ""               # the failure's message when status != 0
+    group: int = 1                  # requests solved together with this one, itself included
 
 
 class Server:
     """csipm_server: `slots` concurrent solves within `hbm_budget` device bytes
     (0: 80% of the free memory); cuda_graphs: each request's iterations as one
-    graph launch."""
+    graph launch; batch > 1: each slot solves up to `batch` requests of one
+    batch class together (csipm_solve_batch, FP64)."""
 
-    def __init__(self, slots=8, hbm_budget=0, device=-1, cuda_graphs=False):
-        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device), int(bool(cuda_graphs)))
+    def __init__(self, slots=8, hbm_budget=0, device=-1, cuda_graphs=False, batch=1):
+        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device), int(bool(cuda_graphs)), int(batch))
         h = ctypes.c_void_p()
         check(lib().csipm_server_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
@@ -101,7 +103,7 @@ class Server:
             z0, miss, beta, _ = self._live.pop(int(r.tag))
             out.append(ServeResult(int(r.tag), int(r.status), r.stats.as_dict(), float(r.queue_ms),
                                    float(r.latency_ms), int(r.footprint), beta,
-                                   r.message.decode(errors="replace")))
+                                   r.message.decode(errors="replace"), int(r.group)))
         return out
 
     def drain(self) -> list[ServeResult]:

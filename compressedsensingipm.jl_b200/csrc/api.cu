@@ -935,9 +935,18 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
         }
         if (cudaMallocFromPoolAsync((void**)&dmiss, sizeof(int64_t) * nm, h->pool, h->stream) != cudaSuccess)
             return bail(CSIPM_ERR_OOM, "out of device memory (missing indices)");
-        // pageable source: the call returns once the indices are staged
-        if (cudaMemcpyAsync(dmiss, prob->host_missing, sizeof(int64_t) * nm, cudaMemcpyHostToDevice, h->stream) !=
-            cudaSuccess) {
+        // through a pinned bounce buffer the handle keeps (an asynchronous
+        // copy: a pageable one would pass through the driver's shared staging);
+        // pageable when no pinned memory is left
+        const void* src = prob->host_missing;
+        size_t pb = 1 << 16;
+        while (pb < sizeof(int64_t) * (size_t)nm) pb <<= 1;
+        if ((h->hmiss = pinned_get(pb)) != nullptr) {
+            h->hmiss_bytes = pb;
+            std::memcpy(h->hmiss, prob->host_missing, sizeof(int64_t) * (size_t)nm);
+            src = h->hmiss;
+        }
+        if (cudaMemcpyAsync(dmiss, src, sizeof(int64_t) * nm, cudaMemcpyHostToDevice, h->stream) != cudaSuccess) {
             cudaFreeAsync(dmiss, h->stream);
             return bail(CSIPM_ERR_CUDA, "missing-index upload failed");
         }

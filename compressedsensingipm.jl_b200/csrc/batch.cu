@@ -267,9 +267,26 @@ struct BatchState {
     BProduct<EpiCG<double>> pc;      // q = A'A p + Db p, p.q
     int gx_elem = 1;
     long long launches = 0;
+    char* hstage = nullptr;       // pinned staging of the tables' uploads
+    size_t hstage_bytes = 0, hstage_used = 0;
     ~BatchState() {
         for (void* p : allocs) cudaFreeAsync(p, st);
         if (hflag) pinned_put(hflag, 64);
+        if (hstage) {
+            cudaStreamSynchronize(st);   // the uploads from it have completed
+            pinned_put(hstage, hstage_bytes);
+        }
+    }
+    // host -> device copy through the pinned staging buffer (asynchronous);
+    // pageable once the buffer is full
+    cudaError_t upload(void* dst, const void* src, size_t bytes) {
+        const size_t at = (hstage_used + 15) & ~(size_t)15;
+        if (hstage && at + bytes <= hstage_bytes) {
+            std::memcpy(hstage + at, src, bytes);
+            hstage_used = at + bytes;
+            return cudaMemcpyAsync(dst, hstage + at, bytes, cudaMemcpyHostToDevice, st);
+        }
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
     }
     template <typename P>
     bool alloc(P** p, size_t count_) {
@@ -413,8 +430,7 @@ int build_product(BatchState& B, BProduct<Epi>& P, const std::vector<csipm_handl
     }
     for (int pass = 0; pass < P.npass; ++pass) {
         if (!B.alloc(&P.tab[pass], t[pass].size())) return CSIPM_ERR_OOM;
-        if (cudaMemcpyAsync(P.tab[pass], t[pass].data(), sizeof(BPass<Epi>) * t[pass].size(),
-                            cudaMemcpyHostToDevice, B.st) != cudaSuccess)
+        if (B.upload(P.tab[pass], t[pass].data(), sizeof(BPass<Epi>) * t[pass].size()) != cudaSuccess)
             return CSIPM_ERR_CUDA;
     }
     return CSIPM_OK;
@@ -501,7 +517,7 @@ int batch_cg_loop(BatchState& B, int which) {
     int since = 0, chunk = 2;
     for (int it = 0; it < BATCH_CG_CAP; ++it) {
         cudaError_t e = batch_product(B, B.pc);
-        if (e != cudaSuccess) return CSIPM_ERR_CUDA;
+        if (e != cudaSuccess) return fail(nullptr, CSIPM_ERR_CUDA, std::string("batch CG product: ") + cudaGetErrorString(e));
         bk_cg_update<<<ge, EW_THREADS, 0, B.st>>>(B.inst, it, which);
         bk_cg_pupdate<<<ge, EW_THREADS, 0, B.st>>>(B.inst, it);
         B.launches += 2;
@@ -511,13 +527,14 @@ int batch_cg_loop(BatchState& B, int which) {
             bk_cg_active<<<1, 256, 0, B.st>>>(B.inst, B.count, B.flag);
             B.launches += 1;
             const int active = read_flag(B);
-            if (active < 0) return CSIPM_ERR_CUDA;
+            if (active < 0) return fail(nullptr, CSIPM_ERR_CUDA, std::string("batch CG loop: ") + cudaGetErrorString(cudaGetLastError()));
             if (active == 0) break;
         }
     }
     bk_cg_post<<<(B.count + 127) / 128, 128, 0, B.st>>>(B.inst, B.count);
     B.launches += 1;
-    return cudaGetLastError() == cudaSuccess ? CSIPM_OK : CSIPM_ERR_CUDA;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CSIPM_OK : fail(nullptr, CSIPM_ERR_CUDA, std::string("batch CG loop: ") + cudaGetErrorString(e));
 }
 
 }  // namespace csipm_internal
@@ -604,7 +621,13 @@ int csipm_solve_batch(csipm_handle* hs_in, int count, double* const* beta_out, c
     if (!B.alloc(&B.inst, count) || !B.alloc(&B.flag, 1)) return done(fail(nullptr, CSIPM_ERR_OOM, "out of device memory"));
     B.hflag = (int*)pinned_get(64);
     if (!B.hflag) return done(fail(nullptr, CSIPM_ERR_OOM, "pinned host allocation failed"));
-    if (cudaMemcpyAsync(B.inst, I.data(), sizeof(BInst) * count, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    {
+        const size_t need = sizeof(BInst) * count + 10 * sizeof(BPass<EpiCG<double>>) * count + 16 * 12;
+        size_t pb = 1 << 16;
+        while (pb < need) pb <<= 1;
+        if ((B.hstage = (char*)pinned_get(pb)) != nullptr) B.hstage_bytes = pb;
+    }
+    if (B.upload(B.inst, I.data(), sizeof(BInst) * count) != cudaSuccess)
         return done(fail(nullptr, CSIPM_ERR_CUDA, "instance table upload failed"));
     {
         int dev = 0, sms = 0, per_sm = 0;
@@ -639,16 +662,22 @@ int csipm_solve_batch(csipm_handle* hs_in, int count, double* const* beta_out, c
     const int g1 = (count + 127) / 128;
     // ---- initial point (as csipm_solve)
     bk_init1<<<ge, EW_THREADS, 0, st>>>(B.inst);
-    if (batch_product(B, B.pq) != cudaSuccess) return done(fail(nullptr, CSIPM_ERR_CUDA, "batch product failed"));
+    {
+        const cudaError_t e = batch_product(B, B.pq);
+        if (e != cudaSuccess) return done(fail(nullptr, CSIPM_ERR_CUDA, std::string("batch product: ") + cudaGetErrorString(e)));
+    }
     bk_init2<<<ge, EW_THREADS, 0, st>>>(B.inst);
     bk_ctl_start<<<g1, 128, 0, st>>>(B.inst, count);
     B.launches += 3;
     int status = CSIPM_OK;
     bool pending = false;
     for (int iter = 0;; ++iter) {
-        if (iter > 0 && batch_product(B, B.pq) != cudaSuccess) {
-            status = fail(nullptr, CSIPM_ERR_CUDA, "batch product failed");
-            break;
+        if (iter > 0) {
+            const cudaError_t e = batch_product(B, B.pq);
+            if (e != cudaSuccess) {
+                status = fail(nullptr, CSIPM_ERR_CUDA, std::string("batch product: ") + cudaGetErrorString(e));
+                break;
+            }
         }
         bk_resid<<<ge, EW_THREADS, 0, st>>>(B.inst, pending ? 1 : 0);
         bk_stop<<<g1, 128, 0, st>>>(B.inst, count);
@@ -674,7 +703,13 @@ int csipm_solve_batch(csipm_handle* hs_in, int count, double* const* beta_out, c
         bk_alpha<<<g1, 128, 0, st>>>(B.inst, count);
         bk_beta_step<<<ge, EW_THREADS, 0, st>>>(B.inst);
         B.launches += 3;
-        if (cudaGetLastError() != cudaSuccess) { status = fail(nullptr, CSIPM_ERR_CUDA, "batch launch failed"); break; }
+        {
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                status = fail(nullptr, CSIPM_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+                break;
+            }
+        }
         pending = true;
     }
     // ---- results
@@ -709,8 +744,9 @@ int csipm_solve_batch(csipm_handle* hs_in, int count, double* const* beta_out, c
         S.solve_ms = ms;
         S.launches = B.launches;
         if (S.status != CSIPM_OK) {
-            h->err = S.status == CSIPM_ERR_NONFINITE ? "non-finite iterate or CG breakdown"
-                                                     : "IPM reached max_iter before the tolerance";
+            h->err = status != CSIPM_OK                  ? std::string(get_last_error())
+                     : S.status == CSIPM_ERR_NONFINITE ? "non-finite iterate or CG breakdown"
+                                                        : "IPM reached max_iter before the tolerance";
             if (first_bad == CSIPM_OK) first_bad = S.status;
         }
         if (stats) stats[k] = S;

@@ -157,8 +157,14 @@ struct csipm_handle_s {
     static constexpr size_t HSLOT_BYTES = sizeof(double) * 64;   // SL_COUNT slots
     static constexpr size_t HCGS_BYTES = 64;                     // >= sizeof(CgScalars)
     static constexpr size_t HCTL_BYTES = 256;                    // >= sizeof(IpmCtl)
+    void* hmiss = nullptr;          // pinned bounce buffer of the missing indices (csipm_create)
+    size_t hmiss_bytes = 0;
 
     ~csipm_handle_s() {
+        if (hmiss) {
+            cudaStreamSynchronize(stream);   // the upload from it has completed
+            pinned_put(hmiss, hmiss_bytes);
+        }
         for (auto& g : cg_exec64)
             if (g) cudaGraphExecDestroy(g);
         for (auto& g : cg_exec32)

@@ -64,24 +64,9 @@ int scratch_address(void** out) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// W_L^e = exp(-2 pi i e / L), e < L, written on the device: sincospi of the
-// exactly reduced angle 2e/L in [0, 2) (one rounding of the quotient, then
-// CUDA's sincospi), so no host table is copied per call.  The handle path's
-// tables are rounded from long double; these agree with them to an ulp or
-// two, far inside the operator's 1e-12 tolerance.
-__global__ void static_twiddle_kernel(int L, double2* __restrict__ out) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < L; e += gridDim.x * blockDim.x) {
-        double s, c;
-        sincospi((double)(2 * (long long)e) / (double)L, &s, &c);
-        out[e] = make_double2(c, -s);
-    }
-}
-
-cudaError_t put_twiddles(int L, double2* dst, cudaStream_t st) {
-    const int blocks = (L + 255) / 256 < 1024 ? (L + 255) / 256 : 1024;
-    static_twiddle_kernel<<<blocks, 256, 0, st>>>(L, dst);
-    return cudaGetLastError();
-}
+// twiddle tables: the handle path's device-built tables (launch_twiddles),
+// so both entry points apply the same operator bit for bit
+cudaError_t put_twiddles(int L, double2* dst, cudaStream_t st) { return launch_twiddles(L, dst, st); }
 
 }  // namespace
 

@@ -644,6 +644,44 @@ inline bool l1d_split(int M, int* P, int* Q) {
     return true;
 }
 
+// W^e = exp(-2 pi i e / L), built on the device from the first octant with
+// the exact symmetries of the roots of unity (sign changes and swaps only):
+//   e in (L/2, L):    W^e = conj W^(L-e)                       (conjugation)
+//   e in [L/4, L/2]:  W^e = -i W^(e-L/4)                       (quarter turn, 4 | L)
+//   e in (L/8, L/4):  W^e = (-Im W^(L/4-e), -Re W^(L/4-e))     (reflection, 8 | L)
+// What remains is computed directly as sincospi(2e/L) (2e/L is one rounding
+// of an exact ratio; for 8 | L it lies in [0, 1/4]).  The table is symmetric
+// bit for bit, as the real-input passes assume.
+__device__ __forceinline__ double2 root_of_unity(long long e, long long L) {
+    bool conj = false, rot = false, refl = false;
+    if (2 * e > L) { e = L - e; conj = true; }
+    if (L % 4 == 0 && 4 * e >= L) { e -= L / 4; rot = true; }
+    if (L % 8 == 0 && 8 * e > L && 4 * e < L) { e = L / 4 - e; refl = true; }
+    double sn, cs;
+    sincospi((double)(2 * e) / (double)L, &sn, &cs);
+    double re = cs, im = -sn;
+    if (refl) { const double r2 = -im; im = -re; re = r2; }
+    if (rot) { const double r2 = im; im = -re; re = r2; }
+    if (conj) im = -im;
+    return make_double2(re, im);
+}
+
+__device__ __forceinline__ void put_root(double2* o, double2 w) { *o = w; }
+__device__ __forceinline__ void put_root(float2* o, double2 w) { *o = make_float2((float)w.x, (float)w.y); }
+
+template <typename C>
+__global__ void twiddle_kernel(int L, C* __restrict__ out) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < L; e += gridDim.x * blockDim.x)
+        put_root(out + e, root_of_unity(e, L));
+}
+
+template <typename C>
+inline cudaError_t launch_twiddles(int L, C* dst, cudaStream_t st) {
+    const int blocks = std::max(1, std::min((L + 255) / 256, 1024));
+    twiddle_kernel<C><<<blocks, 256, 0, st>>>(L, dst);
+    return cudaGetLastError();
+}
+
 template <typename T>
 class FftOperator {
 public:
@@ -701,14 +739,11 @@ public:
         dfree(twQ); twQ = nullptr;
     }
 
+    // twiddle table of L entries, written on the device (stream-ordered: no
+    // host computation, no copy)
     bool upload_table(int L, C** dst, std::string* err) {
-        std::vector<double> t;
-        twiddle_table(L, &t);
-        std::vector<C> h(L);
-        for (int e = 0; e < L; ++e) h[e] = mk((T)t[2 * e], (T)t[2 * e + 1]);
         if (dalloc(dst, L) != cudaSuccess) { *err = "out of device memory (twiddles)"; return false; }
-        // pageable source: returns once staged, so `h` may go out of scope
-        cudaMemcpyAsync(*dst, h.data(), sizeof(C) * L, cudaMemcpyHostToDevice, stream);
+        if (launch_twiddles(L, *dst, stream) != cudaSuccess) { *err = "twiddle kernel launch failed"; return false; }
         return true;
     }
 
@@ -869,32 +904,37 @@ public:
     }
 };
 
-// Opt a kernel into the large dynamic shared-memory carve-out once per
-// (kernel, device).
-inline bool smem_optin_needed(const void* fn, int dev) {
-    static std::mutex mu;
-    static std::set<std::pair<const void*, int>> done;
-    std::lock_guard<std::mutex> lk(mu);
-    return done.insert({fn, dev}).second;
-}
-
+// Opts a kernel into the large dynamic shared-memory carve-out, once per
+// (kernel, device).  The attribute is set under the lock and recorded only
+// after it succeeded, so a thread that launches the kernel concurrently waits
+// for it instead of launching before the opt-in (which fails the launch).
 // The opt-in covers dynamic + static shared memory, so the dynamic limit set
-// here is the device's per-block opt-in maximum minus the kernel's static part.
-template <typename K>
-inline cudaError_t smem_optin(K kernel, size_t smem) {
+// is the device's per-block opt-in maximum minus the kernel's static part.
+inline cudaError_t smem_optin_fn(const void* fn, size_t smem) {
     if (smem <= 48 * 1024) return cudaSuccess;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!smem_optin_needed((const void*)kernel, dev)) return cudaSuccess;
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> limit;   // dynamic bytes set
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = limit.find({fn, dev});
+    if (it != limit.end()) return smem <= it->second ? cudaSuccess : cudaErrorInvalidValue;
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes fa{};
-    e = cudaFuncGetAttributes(&fa, kernel);
+    e = cudaFuncGetAttributes(&fa, fn);
     if (e != cudaSuccess) return e;
     const int dyn = optin - (int)fa.sharedSizeBytes;
-    if ((size_t)dyn < smem) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (dyn < 0 || (size_t)dyn < smem) return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e == cudaSuccess) limit[{fn, dev}] = (size_t)dyn;
+    return e;
+}
+
+template <typename K>
+inline cudaError_t smem_optin(K kernel, size_t smem) {
+    return smem_optin_fn((const void*)kernel, smem);
 }
 
 // Persistent grid: resident CTAs per SM (occupancy API, cached per kernel,
@@ -913,7 +953,10 @@ inline int persistent_grid(const void* fn, int threads, size_t smem, int tiles) 
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (per_sm == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();   // not left for the next launch check to report
+            per_sm = 1;
+        }
         std::lock_guard<std::mutex> lk(mu);
         cache[key] = per_sm;
     }

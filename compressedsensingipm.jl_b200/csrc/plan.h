@@ -1,4 +1,5 @@
-// Host-side FFT planning: radix factorisation and accurate twiddle tables.
+// Host-side FFT planning: radix factorisation.  (Twiddle tables are built on
+// the device: launch_twiddles in operator.cuh.)
 #pragma once
 #include <string>
 #include <vector>
@@ -14,9 +15,6 @@ namespace csipm {
 // cuts the number of shared-memory round trips (320 = 20*16, 160 = 20*8).
 // Any remaining prime becomes a direct-DFT stage.
 bool make_fft_plan(int L, FftPlanDev* out, std::string* err, int max_radix = 8);
-
-// exp(-2*pi*i*e/L) for e = 0..L-1, rounded from long double.
-void twiddle_table(int L, std::vector<double>* re_im);
 
 // True when every stage of `pl` respects the per-thread register budget for
 // `lines` interleaved lines processed by `nthreads` threads.

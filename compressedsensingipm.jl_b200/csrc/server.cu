@@ -11,6 +11,12 @@
 // Handles take their memory from the stream-ordered pool, so creating and
 // destroying them does not stall the other slots.
 //
+// With batching on (csipm_server_options.batch > 1) a slot that admits a
+// request also admits up to batch - 1 more of the same batch class (the
+// dimension count, the long-row 1D passes, missing samples or not), the
+// closest in size first, as far as the budget allows, and solves them
+// together with csipm_solve_batch: one launch per step for all of them.
+//
 // The reference has no serving layer; it solves one recovery per call
 // (src/CompressedSensingIPM.jl:31-36).
 #include <atomic>
@@ -26,12 +32,23 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr int ADMIT_LOOKAHEAD = 16;
+// queued requests a batch looks through for members of its class
+constexpr int BATCH_SCAN = 512;
 
 struct Pending {
     csipm_request req;
     size_t footprint;
+    long long n;          // samples
+    int bclass;           // batch class: requests of one class can share a csipm_solve_batch
     Clock::time_point t_submit;
 };
+
+// dimension count, long-row 1D passes (half-length above the one-CTA row
+// pass's limit), missing samples or not
+int batch_class(const csipm_problem& p) {
+    const bool long1d = p.dim == 1 && p.size[0] / 2 > csipm::L1D_MIN_M;
+    return p.dim * 4 + (long1d ? 2 : 0) + (p.n_missing > 0 ? 1 : 0);
+}
 
 }  // namespace
 
@@ -39,6 +56,7 @@ struct csipm_server_s {
     int device = 0;
     int slots = 0;
     int cuda_graphs = 0;
+    int batch = 1;
     size_t budget = 0;
     size_t in_use = 0;
     bool stopping = false;
@@ -51,7 +69,7 @@ struct csipm_server_s {
     std::vector<std::thread> workers;
 
     void work(int slot);
-    bool take(Pending* out);             // with mu held
+    bool take(std::vector<Pending>* out);    // with mu held
 };
 
 namespace csipm_internal {
@@ -76,27 +94,44 @@ size_t footprint_bytes(int dim, const int* size, int precision, int64_t n_missin
 
 }  // namespace csipm_internal
 
-bool csipm_server_s::take(Pending* out) {
+bool csipm_server_s::take(std::vector<Pending>* out) {
+    out->clear();
     const size_t avail = budget > in_use ? budget - in_use : 0;
     int look = 0;
-    for (auto it = queue.begin(); it != queue.end() && look < ADMIT_LOOKAHEAD; ++it, ++look) {
+    auto head = queue.end();
+    for (auto it = queue.begin(); it != queue.end() && look < ADMIT_LOOKAHEAD; ++it, ++look)
         if (it->footprint <= avail) {
-            *out = *it;
-            in_use += it->footprint;
-            queue.erase(it);
-            return true;
+            head = it;
+            break;
         }
-    }
     // nothing admitted runs and the head still does not fit: admit it alone
     // rather than wait forever (it then fails in csipm_create with OOM if the
     // device really cannot hold it)
-    if (in_use == 0 && !queue.empty()) {
-        *out = queue.front();
-        in_use += out->footprint;
-        queue.pop_front();
-        return true;
+    if (head == queue.end() && in_use == 0 && !queue.empty()) head = queue.begin();
+    if (head == queue.end()) return false;
+    out->push_back(*head);
+    in_use += head->footprint;
+    queue.erase(head);
+    if (batch <= 1) return true;
+    // members of the head's class, closest in size first, while they fit
+    const Pending& h = out->front();
+    std::vector<std::pair<double, int>> cand;
+    int k = 0;
+    for (auto it = queue.begin(); it != queue.end() && k < BATCH_SCAN; ++it, ++k)
+        if (it->bclass == h.bclass) cand.push_back({std::fabs(std::log((double)it->n / (double)h.n)), k});
+    std::stable_sort(cand.begin(), cand.end());
+    std::vector<int> pick;
+    for (const auto& c : cand) {
+        if ((int)(out->size() + pick.size()) >= batch) break;
+        const Pending& q = queue[c.second];
+        if (in_use + q.footprint > budget) continue;
+        in_use += q.footprint;
+        pick.push_back(c.second);
     }
-    return false;
+    std::sort(pick.begin(), pick.end());
+    for (int j : pick) out->push_back(queue[j]);
+    for (auto it = pick.rbegin(); it != pick.rend(); ++it) queue.erase(queue.begin() + *it);
+    return true;
 }
 
 // A slot's pinned host staging buffer for z0 and beta: copies from and to
@@ -125,6 +160,117 @@ static void set_message(csipm_result* r, const char* msg) {
     r->message[sizeof(r->message) - 1] = 0;
 }
 
+// Solves an admitted group on the slot's stream — one request through
+// csipm_solve, several through csipm_solve_batch — and fills one result per
+// member (status, stats, message).  Members stage z0 and beta through one
+// pinned buffer, each at its own offset.
+static void run_group(const std::vector<Pending>& g, int cuda_graphs, cudaStream_t st, cudaMemPool_t pool,
+                      PinnedStage& stage, std::vector<csipm_result>& res) {
+    const int K = (int)g.size();
+    const bool batched = K > 1;
+    const auto t_start = Clock::now();
+    res.assign(K, csipm_result{});
+    std::vector<size_t> off(K + 1, 0);
+    for (int k = 0; k < K; ++k) off[k + 1] = off[k] + (size_t)g[k].n;
+    std::vector<double*> z0(K, nullptr), beta(K, nullptr);
+    std::vector<csipm_handle> h(K, nullptr);
+    std::vector<int> status(K, CSIPM_OK);
+    std::vector<std::string> msg(K);
+    std::vector<char> copied(K, 0);
+    auto failk = [&](int k, int code, const std::string& m) {
+        if (status[k] != CSIPM_OK && status[k] != CSIPM_ERR_IPM_MAXITER && status[k] != CSIPM_ERR_CG_MAXITER) return;
+        status[k] = code;
+        msg[k] = m;
+    };
+    const bool staged = stage.ensure(sizeof(double) * off[K]);
+    for (int k = 0; k < K; ++k) {
+        res[k].tag = g[k].req.tag;
+        res[k].footprint = g[k].footprint;
+        res[k].group = K;
+        res[k].queue_ms = std::chrono::duration<double, std::milli>(t_start - g[k].t_submit).count();
+        const csipm_problem& pr = g[k].req.problem;
+        const size_t bytes = sizeof(double) * (size_t)g[k].n;
+        if (!pool || cudaMallocFromPoolAsync((void**)&z0[k], bytes, pool, st) != cudaSuccess ||
+            cudaMallocFromPoolAsync((void**)&beta[k], bytes, pool, st) != cudaSuccess) {
+            failk(k, CSIPM_ERR_OOM, "out of device memory (staging z0 / beta)");
+            continue;
+        }
+        if (!staged) {
+            failk(k, CSIPM_ERR_OOM, "pinned host allocation failed");
+            continue;
+        }
+        std::memcpy(stage.p + off[k], pr.z0, bytes);
+        if (cudaMemcpyAsync(z0[k], stage.p + off[k], bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            failk(k, CSIPM_ERR_CUDA, "z0 upload failed");
+            continue;
+        }
+        csipm_problem dp = pr;
+        dp.z0 = z0[k];
+        csipm_options o = g[k].req.options;
+        o.stream = st;
+        // a served handle lives for one solve: its graphs are captured for
+        // that one solve, which pays off on the server's say-so only
+        o.cuda_graphs = cuda_graphs;
+        // a batch solves in FP64 (a mixed-precision request gets FP64 iterates,
+        // to its own tolerance)
+        if (batched) o.precision = CSIPM_FP64;
+        const int r = csipm_create(&dp, &o, &h[k]);
+        if (r != CSIPM_OK) {
+            h[k] = nullptr;
+            failk(k, r, csipm_last_error(nullptr));
+        }
+    }
+    if (!batched) {
+        if (h[0] && status[0] == CSIPM_OK) {
+            const int r = csipm_solve(h[0], beta[0], nullptr, &res[0].stats);
+            if (r != CSIPM_OK) failk(0, r, h[0]->err);
+        }
+    } else {
+        std::vector<int> live;
+        std::vector<csipm_handle> hl;
+        std::vector<double*> bl;
+        for (int k = 0; k < K; ++k)
+            if (h[k] && status[k] == CSIPM_OK) {
+                live.push_back(k);
+                hl.push_back(h[k]);
+                bl.push_back(beta[k]);
+            }
+        if (!hl.empty()) {
+            std::vector<csipm_stats> S(hl.size());
+            const int r = csipm_solve_batch(hl.data(), (int)hl.size(), bl.data(), S.data());
+            const std::string batch_err = r != CSIPM_OK ? csipm_last_error(nullptr) : "";
+            for (size_t j = 0; j < live.size(); ++j) {
+                const int k = live[j];
+                res[k].stats = S[j];
+                if (S[j].status != CSIPM_OK) failk(k, S[j].status, h[k]->err.empty() ? batch_err : h[k]->err);
+            }
+        }
+    }
+    for (int k = 0; k < K; ++k) {
+        const int sk = status[k];
+        if (!h[k] || !g[k].req.beta_out) continue;
+        if (sk != CSIPM_OK && sk != CSIPM_ERR_IPM_MAXITER && sk != CSIPM_ERR_CG_MAXITER) continue;
+        if (cudaMemcpyAsync(stage.p + off[k], beta[k], sizeof(double) * (size_t)g[k].n, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+            failk(k, CSIPM_ERR_CUDA, "beta download failed");
+        else
+            copied[k] = 1;
+    }
+    const bool synced = cudaStreamSynchronize(st) == cudaSuccess;
+    for (int k = 0; k < K; ++k) {
+        if (!synced && h[k]) failk(k, CSIPM_ERR_CUDA, "stream synchronisation failed");
+        else if (copied[k]) std::memcpy(g[k].req.beta_out, stage.p + off[k], sizeof(double) * (size_t)g[k].n);
+    }
+    for (int k = 0; k < K; ++k) {
+        if (h[k]) csipm_destroy(h[k]);
+        if (z0[k]) cudaFreeAsync(z0[k], st);
+        if (beta[k]) cudaFreeAsync(beta[k], st);
+        res[k].status = status[k];
+        if (status[k] != CSIPM_OK) set_message(&res[k], msg[k].c_str());
+    }
+    cudaStreamSynchronize(st);
+}
+
 void csipm_server_s::work(int slot) {
     (void)slot;
     cudaSetDevice(device);
@@ -132,86 +278,28 @@ void csipm_server_s::work(int slot) {
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     cudaMemPool_t pool = device_pool(device);
     PinnedStage stage;
+    std::vector<Pending> got;
+    std::vector<csipm_result> res;
     for (;;) {
-        Pending p{};
-        bool got = false;
         {
             std::unique_lock<std::mutex> lk(mu);
+            bool ok = false;
             cv_work.wait(lk, [&] {
-                got = take(&p);
-                return got || (stopping && queue.empty());
+                ok = take(&got);
+                return ok || (stopping && queue.empty());
             });
-            if (!got) break;   // shutting down and nothing left to run
+            if (!ok) break;   // shutting down and nothing left to run
         }
-        const auto t_start = Clock::now();
-        csipm_result res{};
-        res.tag = p.req.tag;
-        res.footprint = p.footprint;
-        res.queue_ms = std::chrono::duration<double, std::milli>(t_start - p.t_submit).count();
-        const csipm_problem& pr = p.req.problem;
-        const long long n = (long long)pr.size[0] * (pr.dim >= 2 ? pr.size[1] : 1) * (pr.dim >= 3 ? pr.size[2] : 1);
-        double* z0 = nullptr;
-        double* beta = nullptr;
-        int status = CSIPM_OK;
-        const char* msg = nullptr;
-        std::string err;
-        if (!pool || cudaMallocFromPoolAsync((void**)&z0, sizeof(double) * n, pool, st) != cudaSuccess ||
-            cudaMallocFromPoolAsync((void**)&beta, sizeof(double) * n, pool, st) != cudaSuccess) {
-            status = CSIPM_ERR_OOM;
-            msg = "out of device memory (staging z0 / beta)";
-        }
-        if (status == CSIPM_OK && !stage.ensure(sizeof(double) * (size_t)n)) {
-            status = CSIPM_ERR_OOM;
-            msg = "pinned host allocation failed";
-        }
-        csipm_handle h = nullptr;
-        if (status == CSIPM_OK) {
-            std::memcpy(stage.p, pr.z0, sizeof(double) * (size_t)n);
-            if (cudaMemcpyAsync(z0, stage.p, sizeof(double) * n, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-                status = CSIPM_ERR_CUDA;
-                msg = "z0 upload failed";
-            }
-        }
-        if (status == CSIPM_OK) {
-            csipm_problem dp = pr;
-            dp.z0 = z0;
-            csipm_options o = p.req.options;
-            o.stream = st;
-            // a served handle lives for one solve: its graphs are captured
-            // for that one solve, which pays off on the server's say-so only
-            o.cuda_graphs = cuda_graphs;
-            status = csipm_create(&dp, &o, &h);
-            if (status != CSIPM_OK) err = csipm_last_error(nullptr);
-        }
-        if (status == CSIPM_OK) {
-            status = csipm_solve(h, beta, nullptr, &res.stats);
-            if (status != CSIPM_OK) err = h->err;
-            if (status == CSIPM_OK || status == CSIPM_ERR_IPM_MAXITER || status == CSIPM_ERR_CG_MAXITER) {
-                if (p.req.beta_out &&
-                    cudaMemcpyAsync(stage.p, beta, sizeof(double) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
-                    status = CSIPM_ERR_CUDA;
-                    msg = "beta download failed";
-                }
-                if (cudaStreamSynchronize(st) != cudaSuccess) {
-                    status = CSIPM_ERR_CUDA;
-                    msg = "stream synchronisation failed";
-                }
-                if (status != CSIPM_ERR_CUDA && p.req.beta_out)
-                    std::memcpy(p.req.beta_out, stage.p, sizeof(double) * (size_t)n);
-            }
-        }
-        if (status != CSIPM_OK) set_message(&res, msg ? msg : err.c_str());
-        if (h) csipm_destroy(h);
-        if (z0) cudaFreeAsync(z0, st);
-        if (beta) cudaFreeAsync(beta, st);
-        cudaStreamSynchronize(st);
-        res.status = status;
-        res.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - p.t_submit).count();
+        run_group(got, cuda_graphs, st, pool, stage, res);
+        const auto t_end = Clock::now();
         {
             std::lock_guard<std::mutex> lk(mu);
-            in_use -= p.footprint;
-            results.push_back(res);
-            ++finished;
+            for (size_t k = 0; k < got.size(); ++k) {
+                res[k].latency_ms = std::chrono::duration<double, std::milli>(t_end - got[k].t_submit).count();
+                in_use -= got[k].footprint;
+                results.push_back(res[k]);
+                ++finished;
+            }
         }
         cv_done.notify_all();
         cv_work.notify_all();   // memory freed: a waiting request may fit now
@@ -240,6 +328,7 @@ int csipm_server_create(const csipm_server_options* opt, csipm_server* out) {
     s->device = dev;
     s->slots = opt && opt->slots > 0 ? opt->slots : 8;
     s->cuda_graphs = opt && opt->cuda_graphs ? 1 : 0;
+    s->batch = opt && opt->batch > 1 ? opt->batch : 1;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = opt && opt->hbm_budget > 0 ? opt->hbm_budget : (size_t)(0.8 * (double)free_b);
@@ -260,6 +349,9 @@ int csipm_server_submit(csipm_server s, const csipm_request* r) {
     Pending p;
     p.req = *r;
     p.footprint = footprint_bytes(r->problem.dim, r->problem.size, r->options.precision, r->problem.n_missing);
+    p.n = (long long)r->problem.size[0] * (r->problem.dim >= 2 ? r->problem.size[1] : 1) *
+          (r->problem.dim >= 3 ? r->problem.size[2] : 1);
+    p.bclass = batch_class(r->problem);
     p.t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -366,6 +366,10 @@ typedef struct {
     int device;                /* CUDA device; -1: the current one */
     int cuda_graphs;           /* 1: each request's solve runs its iterations as one graph launch
                                   (captured per request); 0 (default): plain launches */
+    int batch;                 /* > 1: a slot solves up to `batch` admitted requests of one batch
+                                  class (dimension count, long-row 1D passes, missing samples or
+                                  not), the closest in size to the oldest, together through
+                                  csipm_solve_batch (FP64); 0 or 1 (default): one at a time */
 } csipm_server_options;
 
 typedef struct {
@@ -386,6 +390,8 @@ typedef struct {
     double latency_ms;         /* submission -> result posted (beta_out written) */
     size_t footprint;          /* device bytes the request was admitted with */
     char message[160];         /* the failure's message when status != 0 (truncated), else "" */
+    int group;                 /* requests admitted together with this one, itself included
+                                  (1: solved alone; > 1: one csipm_solve_batch) */
 } csipm_result;
 
 /* Device bytes a handle for this problem holds plus the server's staging of

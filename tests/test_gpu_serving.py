@@ -136,3 +136,54 @@ def test_failed_request_reports_its_message(cuda, problems):
     assert got[0].message == ""
     assert got[1].status == _native.CSIPM_ERR_INVALID
     assert "out of range" in got[1].message
+
+
+def test_batched_serving_matches_alone(cuda, problems):
+    """With batching on, each slot solves up to four admitted requests of one
+    batch class together (csipm_solve_batch, FP64, reference-order passes);
+    every result equals the request solved alone in FP64 up to the order of
+    floating-point sums (beta within 1e-6 relative, IPM iterations within 1),
+    and mixed-precision requests come back with FP64 iterates."""
+    from csipm.serving import Server
+    torch = cuda
+    with Server(slots=2, batch=4) as srv:
+        for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
+            srv.submit(prob.size, prob.z0, prob.lam, prob.missing, tag=k, precision=prec, tol=1e-10,
+                       ipm_cg_rtol=rtol)
+        got = {r.tag: r for r in srv.drain()}
+    assert sorted(got) == list(range(len(MIX)))
+    assert max(r.group for r in got.values()) > 1        # some requests were solved as one batch
+    for k, (prob, (_, _, prec, rtol)) in enumerate(zip(problems, MIX)):
+        r = got[k]
+        assert r.status == 0, (k, r.stats, r.message)
+        alone = _alone(torch, prob, "fp64", rtol)
+        b = alone.beta.cpu().numpy()
+        assert np.linalg.norm(r.beta - b) <= 1e-6 * np.linalg.norm(b), k
+        assert abs(r.stats["ipm_iter"] - alone.stats["ipm_iter"]) <= 1
+        assert r.latency_ms >= r.queue_ms >= 0.0
+
+
+def test_batched_serving_member_failures(cuda, problems):
+    """In a batch, a request the library rejects (a missing index out of
+    range) and one capped at 2 iterations return their own status and
+    message; the members beside them converge."""
+    from csipm import _native
+    from csipm.serving import Server
+    good = problems[2]                      # 2D 64 x 64
+    other = problems[7]                     # 2D 120 x 64
+    big = problems[6]                       # 3D 48^3, another batch class: keeps the one slot busy
+    n = int(np.prod(good.size))
+    with Server(slots=1, batch=4) as srv:
+        srv.submit(big.size, big.z0, big.lam, big.missing, tag=9, tol=1e-10, ipm_cg_rtol=1e-8)
+        srv.submit(good.size, good.z0, good.lam, good.missing, tag=0, tol=1e-8)
+        srv.submit(good.size, good.z0, good.lam, np.array([0, n + 5], dtype=np.int64), tag=1)
+        srv.submit(other.size, other.z0, other.lam, other.missing, tag=2, tol=1e-8, max_iter=2)
+        srv.submit(other.size, other.z0, other.lam, other.missing, tag=3, tol=1e-8)
+        got = {r.tag: r for r in srv.drain()}
+    assert got[9].status == 0
+    assert all(got[k].group == 4 for k in range(4))         # the four 2D requests formed one batch
+    assert got[0].status == 0 and got[3].status == 0
+    assert got[0].message == "" and got[3].message == ""
+    assert got[1].status == _native.CSIPM_ERR_INVALID and "out of range" in got[1].message
+    assert got[2].status == _native.CSIPM_ERR_IPM_MAXITER and got[2].stats["ipm_iter"] == 2
+    assert "max_iter" in got[2].message
