@@ -80,6 +80,27 @@ mutable struct CsipmStats                # csipm_stats
 end
 CsipmStats() = CsipmStats(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
 
+# csipm_stats as an immutable (inline) row, for arrays of statistics
+struct CsipmStatsRow
+    status::Cint
+    ipm_iter::Cint
+    cg_iter::Cint
+    matvecs::Cint
+    refinements::Cint
+    gap::Cdouble
+    obj::Cdouble
+    lasso_obj::Cdouble
+    mu::Cdouble
+    dual_inf::Cdouble
+    solve_ms::Cdouble
+    launches::Clonglong
+    fallbacks::Cint
+    resid_pass_ms::Cdouble
+    resid_pass_bytes::Cdouble
+    resid_pass_launches::Cint
+    graph_iters::Cint
+end
+
 function csipm_check(st, h=C_NULL)
     st == 0 && return nothing
     msg = unsafe_string(ccall((:csipm_last_error, libcsipm), Cstring, (Ptr{Cvoid},), h))
@@ -417,6 +438,24 @@ function device_ipm_solve!(nlp::CsipmNLP)
                nlp.h.ptr, beta, c, stats)
     st in (0, -8) || csipm_check(st, nlp.h.ptr)   # -8: max_iter reached (the iterate is still returned)
     return beta, c, stats[]
+end
+
+# Several recoveries solved together on the device (csipm_solve_batch): one
+# kernel launch per step for all of them, FP64.  The models share the
+# dimension count, the long-row 1D passes and the presence of missing
+# samples; sizes, lambda and options are their own.  Returns each beta and
+# its statistics (status per instance: 0 converged, -8 max_iter, ...).
+function device_ipm_solve_batch!(nlps::AbstractVector{<:CsipmNLP})
+    n = length(nlps)
+    betas = [CUDA.zeros(Float64, nlp.nβ) for nlp in nlps]
+    handles = Ptr{Cvoid}[nlp.h.ptr for nlp in nlps]
+    outs = Ptr{Cdouble}[Ptr{Cdouble}(reinterpret(UInt, pointer(b))) for b in betas]
+    stats = Vector{CsipmStatsRow}(undef, n)
+    st = GC.@preserve betas ccall((:csipm_solve_batch, libcsipm), Cint,
+                                  (Ptr{Ptr{Cvoid}}, Cint, Ptr{Ptr{Cdouble}}, Ptr{CsipmStatsRow}),
+                                  handles, n, outs, stats)
+    st in (0, -6, -7, -8) || csipm_check(st, C_NULL)   # per-instance failures are in stats[k].status
+    return betas, stats
 end
 
 # ============================================================ Gondzio pair
