@@ -83,6 +83,9 @@ def parse():
                     help="plain kernel launches instead of CUDA graphs (launch-list profiling sees every kernel)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default pass variants instead of the per-size autotuner (profilers distort its timings)")
+    ap.add_argument("--solves-only", action="store_true",
+                    help="run the warm-up and timed headline solves only, print their time and exit (the command "
+                         "for launch lists)")
     ap.add_argument("--passes-only", action="store_true",
                     help="build the handle, launch each pass of one CG product twice (csipm_profile_passes, "
                          "reps=1), print the pass list and exit: the small command for kernel captures")
@@ -384,7 +387,15 @@ def run_ours(args):
         rp = {k: sum(s_[k] for s_ in stats) for k in ("resid_pass_ms", "resid_pass_bytes", "resid_pass_launches")}
         return D.max(e0.elapsed_time(e1) / steps), stats[-1], clk, rp
 
-    ms, last, clk, rp = timed(nlp, args.steps, args.warmup, True)
+    ms, last, clk, rp = timed(nlp, args.steps, args.warmup, args.solves_only is False)
+    if args.solves_only:
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "precision": args.precision, "ms_per_solve": round(ms, 3),
+                              "ipm_iter": last["ipm_iter"], "cg_iter": last["cg_iter"], "launches": last["launches"]}),
+                  flush=True)
+        nlp.op_fft.close()
+        D.close()
+        return
     beta_main = sol[:N].clone()
 
     # ---- accuracy oracle: a tight FP64 device solve of the same problem

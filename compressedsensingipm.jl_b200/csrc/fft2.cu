@@ -18,11 +18,33 @@ cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, c
     return cudaErrorInvalidValue;
 }
 
+// The bulk-staged persistent kernel for whole tiles of the spectrum-to-
+// spectrum pass; false when the pass does not qualify (then the plain one).
+template <typename T, int AA, int BB, bool MASK>
+bool launch_row2b(const PassArgs<T>& a, cudaStream_t st, cudaError_t* err) {
+    using Sh = Row2Shape<T, AA, BB>;
+    const size_t tile_bytes = (size_t)Sh::ROWS * a.g.ld1 * sizeof(cplx_t<T>);
+    if (a.nrows % Sh::ROWS || tile_bytes % 16 || ((uintptr_t)a.spec & 15) || a.g.ld1 < Sh::M + 1) return false;
+    auto k = row2b_kernel<T, AA, BB, MASK>;
+    const int threads = Sh::ROWS * Sh::NTL;
+    *err = smem_optin_fn((const void*)k, tile_bytes, true);
+    if (*err != cudaSuccess) return true;
+    const int ntiles = a.nrows / Sh::ROWS;
+    const int grid = persistent_grid((const void*)k, threads, tile_bytes, ntiles);
+    k<<<grid, threads, tile_bytes, st>>>(a, ntiles);
+    *err = cudaGetLastError();
+    return true;
+}
+
 template <typename T, int IN, int OUT, bool MASK>
 cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st) {
 #define CSIPM_R2(AA, BB)                                                                                   \
     if (A == AA && B == BB) {                                                                              \
         using Sh = Row2Shape<T, AA, BB>;                                                                   \
+        if (IN == IN_SPEC && OUT == OUT_SPEC) {                                                            \
+            cudaError_t e = cudaSuccess;                                                                   \
+            if (launch_row2b<T, AA, BB, MASK>(a, st, &e)) return e;                                        \
+        }                                                                                                  \
         const dim3 grid((a.nrows + Sh::ROWS - 1) / Sh::ROWS, 1, 1);                                        \
         row2_kernel<T, AA, BB, IN, OUT, MASK><<<grid, Sh::ROWS * Sh::NTL, 0, st>>>(a);                     \
         return cudaGetLastError();                                                                         \

@@ -14,6 +14,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "bulk.cuh"
 #include "fft_device.cuh"
 #include "operator.cuh"
 
@@ -280,6 +281,15 @@ template <typename T, int A, int B> struct Row2Shape {
     static constexpr int BY_REGS = 65536 / (ROWS * NTL * 128);
     static constexpr int MINB_RAW = BY_SMEM < BY_REGS ? BY_SMEM : BY_REGS;
     static constexpr int MINB = (sizeof(T) != 8 || A == 16 || MINB_RAW < 1) ? 1 : MINB_RAW;
+    // Bulk-staged variant (row2b_kernel): one tile buffer of ROWS rows of
+    // M+1 values beside the exchange area; resident CTAs per SM: as many as
+    // shared memory holds at up to ~100 (FP32) / ~168 (FP64) registers per
+    // thread, at most 6.
+    static constexpr int TILE = ROWS * (M + 1) * (int)sizeof(cplx_t<T>);
+    static constexpr int BY_SMEM_B = (228 * 1024) / (SMEM + TILE + 1024);
+    static constexpr int BY_REGS_B = 65536 / (ROWS * NTL * (sizeof(T) == 8 ? 168 : 100));
+    static constexpr int MINB_B0 = BY_SMEM_B < BY_REGS_B ? BY_SMEM_B : BY_REGS_B;
+    static constexpr int MINB_B = MINB_B0 < 1 ? 1 : (MINB_B0 > 6 ? 6 : MINB_B0);
 };
 
 // Two thread mappings share the CTA: the B-task phases (inverse step 1,
@@ -408,6 +418,172 @@ row2_kernel(PassArgs<T> a) {
                 rowp[k] = r2c_post(P[k], P[M - k], tw[k]);
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------- row pass, bulk-staged
+// The spectrum-to-spectrum row pass (C2R, scale + mask, R2C) as a persistent
+// kernel whose input rows arrive by bulk asynchronous copies (cp.async.bulk,
+// completed on an mbarrier).  A tile is ROWS consecutive rows, which are
+// contiguous in the half spectrum (pitch ld1), so one copy brings a tile.
+// Once the first step of the inverse transform has read the tile into
+// registers, the buffer is free and thread 0 issues the copy of the CTA's
+// next tile; it lands while the rest of this tile is transformed, so the
+// loads of a tile no longer stall the SM at its start (the plain kernel's
+// long-scoreboard stalls).  Results go out with ordinary coalesced stores.
+// The host uses it for whole tiles only (nrows a multiple of ROWS, tile bytes
+// a multiple of 16, 16-byte aligned spectrum).
+//
+// Every wait is bounded: if a tile's copy has not completed after
+// ROW2B_WAIT_LIMIT polls, the CTA writes NaN into that tile's rows (so the
+// solve reports a non-finite iterate), counts the event in
+// g_row2b_timeouts and returns.
+constexpr int ROW2B_WAIT_LIMIT = 1 << 22;
+static __device__ int g_row2b_timeouts;
+
+template <typename T, int A, int B, bool MASK>
+__global__ void __launch_bounds__(Row2Shape<T, A, B>::ROWS * Row2Shape<T, A, B>::NTL, Row2Shape<T, A, B>::MINB_B)
+row2b_kernel(PassArgs<T> a, int ntiles) {
+    using C = cplx_t<T>;
+    using Sh = Row2Shape<T, A, B>;
+    constexpr int M = Sh::M;
+    constexpr int NTL = Sh::NTL;
+    constexpr int R = Sh::ROWS;
+    static_assert(A <= B, "row pass factors are ordered A <= B");
+    if (a.skip && *a.skip) return;
+    __shared__ C S[R * Sh::PER_ROW];
+    __shared__ __align__(8) uint64_t full;
+    __shared__ int s_ok;
+    extern __shared__ __align__(16) unsigned char row2b_dyn[];
+    C* buf = reinterpret_cast<C*>(row2b_dyn);
+    const int ld = a.g.ld1;
+    const size_t tile_elems = (size_t)R * ld;
+    const uint32_t tile_bytes = (uint32_t)(tile_elems * sizeof(C));
+    // B-task mapping
+    const int r = threadIdx.x / NTL, t = threadIdx.x % NTL;
+    C* X = S + r * Sh::PER_ROW;
+    C* P = X + Sh::XC;
+    const C* rowp = buf + (size_t)r * ld;
+    // A-task mapping
+    const bool ta = threadIdx.x < R * A;
+    const int ra = threadIdx.x / A, s = threadIdx.x % A;
+    C* XA = S + (ta ? ra : 0) * Sh::PER_ROW;
+    const C* __restrict__ tw = a.tw;
+    const T sc = (T)a.scale;
+    const uint32_t bar = smem_u32(&full);
+    const uint32_t dst = smem_u32(buf);
+
+    int tile = blockIdx.x;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+        if (tile < ntiles) {
+            mbar_arrive_expect_tx(bar, tile_bytes);
+            bulk_g2s(dst, a.spec + (size_t)tile * tile_elems, tile_bytes, bar);
+        }
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    for (; tile < ntiles; tile += gridDim.x, parity ^= 1u) {
+        // thread 0 waits (bounded) and tells the others; then every thread
+        // observes the completed phase itself, which returns at once
+        if (threadIdx.x == 0) s_ok = mbar_wait_bounded(bar, parity, ROW2B_WAIT_LIMIT) ? 1 : 0;
+        __syncthreads();
+        if (!s_ok) {
+            if (threadIdx.x == 0) atomicAdd(&g_row2b_timeouts, 1);
+            const T nan = (T)__int_as_float(0x7fc00000);
+            C* out = a.spec + (size_t)tile * tile_elems;
+            for (size_t e = threadIdx.x; e < tile_elems; e += blockDim.x) out[e] = mk(nan, nan);
+            return;
+        }
+        mbar_try_wait(bar, parity);
+        const int row = tile * R + r;
+        // ---- inverse step 1 (B-task t): C2R pre-processing from the tile
+        {
+            C v[A];
+#pragma unroll
+            for (int q = 0; q < A; ++q) {
+                const int x = t + B * q;
+                v[q] = c2r_pre(rowp[x], rowp[M - x], tw[x]);
+            }
+            Dft<A, true, T>::run(v);
+#pragma unroll
+            for (int ka = 0; ka < A; ++ka) {
+                C w = v[ka];
+                const int e = t * ka;
+                if (e) w = cmulc(w, tw[2 * e]);
+                X[ka * (B + 1) + t] = w;
+            }
+        }
+        __syncthreads();
+        // the tile buffer is free: bring the next tile while this one is transformed
+        if (threadIdx.x == 0) {
+            const int next = tile + gridDim.x;
+            if (next < ntiles) {
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(bar, tile_bytes);
+                bulk_g2s(dst, a.spec + (size_t)next * tile_elems, tile_bytes, bar);
+            }
+        }
+        // ---- inverse step 2 (A-task s)
+        C z[B];
+        if (ta) {
+#pragma unroll
+            for (int q = 0; q < B; ++q) z[q] = XA[s * (B + 1) + q];
+            Dft<B, true, T>::run(z);
+        }
+        __syncthreads();   // the exchange area is reused by the forward transform
+        // ---- scale and mask the real samples (x[2n], x[2n+1]) = z[n], n = s + A*kb
+        const int rowa = tile * R + ra;
+        if (ta) {
+#pragma unroll
+            for (int kb = 0; kb < B; ++kb) {
+                const int n = s + A * kb;
+                C y = z[kb];
+                y.x *= sc;
+                y.y *= sc;
+                if (MASK) {
+                    const uint32_t w = a.maskw[(size_t)rowa * a.wpr + (n >> 4)];
+                    const int sh = (2 * n) & 31;
+                    if (!((w >> sh) & 1u)) y.x = (T)0;
+                    if (!((w >> (sh + 1)) & 1u)) y.y = (T)0;
+                }
+                z[kb] = y;
+            }
+            // ---- forward transform with factors (B, A): step 1 (A-task s)
+            Dft<B, false, T>::run(z);
+#pragma unroll
+            for (int kb = 0; kb < B; ++kb) {
+                C w = z[kb];
+                const int e = s * kb;
+                if (e) w = cmul(w, tw[2 * e]);
+                XA[kb * (A + 1) + s] = w;
+            }
+        }
+        __syncthreads();
+        // step 2 (B-task t): outputs Z[t + B*ka]
+        {
+            C u[A];
+#pragma unroll
+            for (int q = 0; q < A; ++q) u[q] = X[t * (A + 1) + q];
+            Dft<A, false, T>::run(u);
+#pragma unroll
+            for (int ka = 0; ka < A; ++ka) P[t + B * ka] = u[ka];
+        }
+        __syncthreads();
+        // ---- R2C post-processing and coalesced store of the M+1 values
+        {
+            C* rowg = a.spec + (size_t)row * ld;
+            for (int k = t; k <= M; k += NTL) {
+                if (k == 0 || k == M) {
+                    const C z0 = P[0];
+                    rowg[k] = k == 0 ? r2c_post(z0, z0, tw[0]) : mk((T)2 * (z0.x - z0.y), (T)0);
+                } else {
+                    rowg[k] = r2c_post(P[k], P[M - k], tw[k]);
+                }
+            }
+        }
+        __syncthreads();   // P and the exchange area are reused by the next tile
     }
 }
 

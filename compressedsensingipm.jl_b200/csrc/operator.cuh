@@ -910,8 +910,10 @@ public:
 // for it instead of launching before the opt-in (which fails the launch).
 // The opt-in covers dynamic + static shared memory, so the dynamic limit set
 // is the device's per-block opt-in maximum minus the kernel's static part.
-inline cudaError_t smem_optin_fn(const void* fn, size_t smem) {
-    if (smem <= 48 * 1024) return cudaSuccess;
+// `always`: opt in even when the dynamic part alone is within 48 KB (a
+// kernel whose static and dynamic shared memory together exceed it).
+inline cudaError_t smem_optin_fn(const void* fn, size_t smem, bool always = false) {
+    if (smem <= 48 * 1024 && !always) return cudaSuccess;
     int dev = 0;
     cudaGetDevice(&dev);
     static std::mutex mu;
