@@ -27,11 +27,12 @@ bool launch_row2b(const PassArgs<T>& a, cudaStream_t st, cudaError_t* err) {
     if (a.nrows % Sh::ROWS || tile_bytes % 16 || ((uintptr_t)a.spec & 15) || a.g.ld1 < Sh::M + 1) return false;
     auto k = row2b_kernel<T, AA, BB, MASK>;
     const int threads = Sh::ROWS * Sh::NTL;
-    *err = smem_optin_fn((const void*)k, tile_bytes, true);
+    const size_t dyn = tile_bytes + 2 * (size_t)Sh::M * sizeof(cplx_t<T>);   // tile + twiddle tables
+    *err = smem_optin_fn((const void*)k, dyn, true);
     if (*err != cudaSuccess) return true;
     const int ntiles = a.nrows / Sh::ROWS;
-    const int grid = persistent_grid((const void*)k, threads, tile_bytes, ntiles);
-    k<<<grid, threads, tile_bytes, st>>>(a, ntiles);
+    const int grid = persistent_grid((const void*)k, threads, dyn, ntiles);
+    k<<<grid, threads, dyn, st>>>(a, ntiles);
     *err = cudaGetLastError();
     return true;
 }

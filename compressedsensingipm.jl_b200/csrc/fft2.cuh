@@ -282,10 +282,11 @@ template <typename T, int A, int B> struct Row2Shape {
     static constexpr int MINB_RAW = BY_SMEM < BY_REGS ? BY_SMEM : BY_REGS;
     static constexpr int MINB = (sizeof(T) != 8 || A == 16 || MINB_RAW < 1) ? 1 : MINB_RAW;
     // Bulk-staged variant (row2b_kernel): one tile buffer of ROWS rows of
-    // M+1 values beside the exchange area; resident CTAs per SM: as many as
+    // M+1 values and two M-entry twiddle tables beside the exchange area;
+    // resident CTAs per SM: as many as
     // shared memory holds at up to ~100 (FP32) / ~168 (FP64) registers per
     // thread, at most 6.
-    static constexpr int TILE = ROWS * (M + 1) * (int)sizeof(cplx_t<T>);
+    static constexpr int TILE = (ROWS * (M + 1) + 2 * M) * (int)sizeof(cplx_t<T>);
     static constexpr int BY_SMEM_B = (228 * 1024) / (SMEM + TILE + 1024);
     static constexpr int BY_REGS_B = 65536 / (ROWS * NTL * (sizeof(T) == 8 ? 168 : 100));
     static constexpr int MINB_B0 = BY_SMEM_B < BY_REGS_B ? BY_SMEM_B : BY_REGS_B;
@@ -452,12 +453,20 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
     static_assert(A <= B, "row pass factors are ordered A <= B");
     if (a.skip && *a.skip) return;
     __shared__ C S[R * Sh::PER_ROW];
+    // the twiddles of the two inner steps, laid out for their readers: the
+    // inverse step 1 reads W^(t*ka) with consecutive t across lanes, the
+    // forward step 1 W^(s*kb) with consecutive s; read from the N1-th root
+    // table those are strided (a line per lane), which made the L1 pipe the
+    // pass's bound
     __shared__ __align__(8) uint64_t full;
     __shared__ int s_ok;
+    // dynamic: the tile buffer (R rows at pitch ld1), then T1 and T2
     extern __shared__ __align__(16) unsigned char row2b_dyn[];
     C* buf = reinterpret_cast<C*>(row2b_dyn);
     const int ld = a.g.ld1;
     const size_t tile_elems = (size_t)R * ld;
+    C* T1 = buf + tile_elems;   // T1[ka*B + t] = W_M^(t*ka)
+    C* T2 = T1 + M;             // T2[kb*A + s] = W_M^(s*kb)
     const uint32_t tile_bytes = (uint32_t)(tile_elems * sizeof(C));
     // B-task mapping
     const int r = threadIdx.x / NTL, t = threadIdx.x % NTL;
@@ -473,6 +482,12 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
     const uint32_t bar = smem_u32(&full);
     const uint32_t dst = smem_u32(buf);
 
+    for (int e = threadIdx.x; e < M; e += blockDim.x) {
+        const int ka = e / B, tt = e % B;
+        T1[e] = tw[2 * ((tt * ka) % M)];
+        const int kb = e / A, ss = e % A;
+        T2[e] = tw[2 * ((ss * kb) % M)];
+    }
     int tile = blockIdx.x;
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -510,8 +525,7 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
 #pragma unroll
             for (int ka = 0; ka < A; ++ka) {
                 C w = v[ka];
-                const int e = t * ka;
-                if (e) w = cmulc(w, tw[2 * e]);
+                if (t * ka) w = cmulc(w, T1[ka * B + t]);
                 X[ka * (B + 1) + t] = w;
             }
         }
@@ -555,8 +569,7 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
 #pragma unroll
             for (int kb = 0; kb < B; ++kb) {
                 C w = z[kb];
-                const int e = s * kb;
-                if (e) w = cmul(w, tw[2 * e]);
+                if (s * kb) w = cmul(w, T2[kb * A + s]);
                 XA[kb * (A + 1) + s] = w;
             }
         }
