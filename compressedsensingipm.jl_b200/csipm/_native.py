@@ -108,7 +108,7 @@ class AdmmStats(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("device", ctypes.c_int),
-                ("cuda_graphs", ctypes.c_int), ("batch", ctypes.c_int)]
+                ("cuda_graphs", ctypes.c_int), ("batch", ctypes.c_int), ("batch_max_n", ctypes.c_longlong)]
 
 
 class Request(ctypes.Structure):

@@ -50,10 +50,12 @@ class Server:
     """csipm_server: `slots` concurrent solves within `hbm_budget` device bytes
     (0: 80% of the free memory); cuda_graphs: each request's iterations as one
     graph launch; batch > 1: each slot solves up to `batch` requests of one
-    batch class together (csipm_solve_batch, FP64)."""
+    batch class together (csipm_solve_batch, FP64); batch_max_n > 0: requests
+    of more samples are solved alone."""
 
-    def __init__(self, slots=8, hbm_budget=0, device=-1, cuda_graphs=False, batch=1):
-        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device), int(bool(cuda_graphs)), int(batch))
+    def __init__(self, slots=8, hbm_budget=0, device=-1, cuda_graphs=False, batch=1, batch_max_n=0):
+        o = _native.ServerOptions(int(slots), int(hbm_budget), int(device), int(bool(cuda_graphs)), int(batch),
+                                  int(batch_max_n))
         h = ctypes.c_void_p()
         check(lib().csipm_server_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h

@@ -16,6 +16,9 @@
 // dimension count, the long-row 1D passes, missing samples or not), the
 // closest in size first, as far as the budget allows, and solves them
 // together with csipm_solve_batch: one launch per step for all of them.
+// Requests above batch_max_n samples (when set) are solved alone: they fill
+// the GPU by themselves, and alone they keep their precision (a batch runs
+// FP64).
 //
 // The reference has no serving layer; it solves one recovery per call
 // (src/CompressedSensingIPM.jl:31-36).
@@ -57,6 +60,7 @@ struct csipm_server_s {
     int slots = 0;
     int cuda_graphs = 0;
     int batch = 1;
+    long long batch_max_n = 0;
     size_t budget = 0;
     size_t in_use = 0;
     bool stopping = false;
@@ -113,12 +117,15 @@ bool csipm_server_s::take(std::vector<Pending>* out) {
     in_use += head->footprint;
     queue.erase(head);
     if (batch <= 1) return true;
-    // members of the head's class, closest in size first, while they fit
+    // members of the head's class, closest in size first, while they fit;
+    // requests above batch_max_n samples are solved alone
     const Pending& h = out->front();
+    if (batch_max_n > 0 && h.n > batch_max_n) return true;
     std::vector<std::pair<double, int>> cand;
     int k = 0;
     for (auto it = queue.begin(); it != queue.end() && k < BATCH_SCAN; ++it, ++k)
-        if (it->bclass == h.bclass) cand.push_back({std::fabs(std::log((double)it->n / (double)h.n)), k});
+        if (it->bclass == h.bclass && (batch_max_n <= 0 || it->n <= batch_max_n))
+            cand.push_back({std::fabs(std::log((double)it->n / (double)h.n)), k});
     std::stable_sort(cand.begin(), cand.end());
     std::vector<int> pick;
     for (const auto& c : cand) {
@@ -329,6 +336,7 @@ int csipm_server_create(const csipm_server_options* opt, csipm_server* out) {
     s->slots = opt && opt->slots > 0 ? opt->slots : 8;
     s->cuda_graphs = opt && opt->cuda_graphs ? 1 : 0;
     s->batch = opt && opt->batch > 1 ? opt->batch : 1;
+    s->batch_max_n = opt && opt->batch_max_n > 0 ? opt->batch_max_n : 0;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = opt && opt->hbm_budget > 0 ? opt->hbm_budget : (size_t)(0.8 * (double)free_b);

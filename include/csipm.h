@@ -370,6 +370,8 @@ typedef struct {
                                   class (dimension count, long-row 1D passes, missing samples or
                                   not), the closest in size to the oldest, together through
                                   csipm_solve_batch (FP64); 0 or 1 (default): one at a time */
+    long long batch_max_n;     /* with batch > 1: requests of more samples are solved alone (they
+                                  fill the GPU by themselves and keep their precision); 0: no limit */
 } csipm_server_options;
 
 typedef struct {

@@ -187,3 +187,21 @@ def test_batched_serving_member_failures(cuda, problems):
     assert got[1].status == _native.CSIPM_ERR_INVALID and "out of range" in got[1].message
     assert got[2].status == _native.CSIPM_ERR_IPM_MAXITER and got[2].stats["ipm_iter"] == 2
     assert "max_iter" in got[2].message
+
+
+def test_batched_serving_size_cap(cuda, problems):
+    """batch_max_n: a request above the cap is solved alone (group 1) even
+    with requests of its class waiting; those below the cap still batch."""
+    from csipm.serving import Server
+    blocker = problems[3]                   # 2D 96 x 128: keeps the one slot busy while the rest queue
+    big = problems[6]                       # 3D 48^3 = 110592 samples, above the cap
+    small = [problems[4], problems[8], problems[5]]   # 3D 32^3, 16^3, 32x64x24
+    with Server(slots=1, batch=4, batch_max_n=60000) as srv:
+        srv.submit(blocker.size, blocker.z0, blocker.lam, blocker.missing, tag=9, tol=1e-10, ipm_cg_rtol=1e-8)
+        srv.submit(big.size, big.z0, big.lam, big.missing, tag=0, tol=1e-8)
+        for k, p in enumerate(small):
+            srv.submit(p.size, p.z0, p.lam, p.missing, tag=1 + k, tol=1e-8)
+        got = {r.tag: r for r in srv.drain()}
+    assert all(r.status == 0 for r in got.values()), {t: r.message for t, r in got.items()}
+    assert got[0].group == 1
+    assert all(got[t].group == 3 for t in (1, 2, 3))
