@@ -54,7 +54,7 @@ struct BPass {
     const double* src;
     Epi epi;
     const double2* twN;
-    int P, Q, RB, pad;
+    int P, Q, RB, TB;
 };
 
 // ------------------------------------------------------------------ element kernels
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256) bk_row(const BPass<Epi>* __restrict__ B) 
 template <class Epi>
 __global__ void __launch_bounds__(256) bk_l1d_first(const BPass<Epi>* __restrict__ B) {
     const BPass<Epi>& e = B[blockIdx.y];
-    l1d_first_kernel_body<double, double>(e.a, e.src, e.twN, e.P, e.Q);
+    l1d_first_kernel_body<double, double>(e.a, e.src, e.twN, e.P, e.Q, e.TB);
 }
 
 template <bool MASK, class Epi>
@@ -332,7 +332,7 @@ int build_product(BatchState& B, BProduct<Epi>& P, const std::vector<csipm_handl
     std::vector<std::vector<BPass<Epi>>> t;
     const double C = sizeof(double2);
     auto add = [&](int pass, const PassArgs<double>& a, const double* src, const Epi& e, const double2* twN, int Pp,
-                   int Qq, int RB) {
+                   int Qq, int RB, int TB = 0) {
         if ((int)t.size() <= pass) t.resize(pass + 1);
         BPass<Epi> bp{};
         bp.a = a;
@@ -342,6 +342,7 @@ int build_product(BatchState& B, BProduct<Epi>& P, const std::vector<csipm_handl
         bp.P = Pp;
         bp.Q = Qq;
         bp.RB = RB;
+        bp.TB = TB;
         t[pass].push_back(bp);
     };
     for (int k = 0; k < K; ++k) {
@@ -358,9 +359,9 @@ int build_product(BatchState& B, BProduct<Epi>& P, const std::vector<csipm_handl
             P.gx[0] = std::max(P.gx[0], op.row_cfg.tiles);
         } else if (P.kind == PK_1DL) {
             PassArgs<double> a0 = l1d_args(op, false, 1.0, skip[k]);
-            add(0, a0, x[k], epi[k], op.tw1, op.l1P, op.l1Q, op.l1RB);
-            P.smem[0] = std::max(P.smem[0], (size_t)(2 * op.l1Q * L1D_TB * C));
-            P.gx[0] = std::max(P.gx[0], (op.l1P + L1D_TB - 1) / L1D_TB);
+            add(0, a0, x[k], epi[k], op.tw1, op.l1P, op.l1Q, op.l1RB, op.l1TB);
+            P.smem[0] = std::max(P.smem[0], (size_t)(2 * op.l1Q * op.l1TB * C));
+            P.gx[0] = std::max(P.gx[0], (op.l1P + op.l1TB - 1) / op.l1TB);
             PassArgs<double> a1 = l1d_args(op, true, sc, skip[k]);
             add(1, a1, nullptr, epi[k], op.tw1, op.l1P, op.l1Q, op.l1RB);
             P.smem[1] = std::max(P.smem[1], (size_t)(2 * op.l1P * op.l1RB * C));

@@ -24,13 +24,13 @@
 namespace csipm {
 
 // ---------------------------------------------------------------- first pass
+// TB lines k1 per CTA (l1d_tiles), interleaved in shared memory as buf[x*TB + b].
 template <typename T, typename TS>
 __device__ __forceinline__ void l1d_first_kernel_body(PassArgs<T> a, const TS* __restrict__ src,
-                                                        const cplx_t<T>* __restrict__ twN, int P, int Q) {
+                                                        const cplx_t<T>* __restrict__ twN, int P, int Q, int TB) {
     using C = cplx_t<T>;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int TB = L1D_TB;
     C* buf = reinterpret_cast<C*>(smem_raw);
     C* work = buf + Q * TB;
     __shared__ int s_rad[FFT_MAX_STAGES];
@@ -64,8 +64,8 @@ __device__ __forceinline__ void l1d_first_kernel_body(PassArgs<T> a, const TS* _
 }
 template <typename T, typename TS>
 __global__ void __launch_bounds__(256) l1d_first_kernel(PassArgs<T> a, const TS* __restrict__ src,
-                                                        const cplx_t<T>* __restrict__ twN, int P, int Q) {
-    l1d_first_kernel_body<T, TS>(a, src, twN, P, Q);
+                                                        const cplx_t<T>* __restrict__ twN, int P, int Q, int TB) {
+    l1d_first_kernel_body<T, TS>(a, src, twN, P, Q, TB);
 }
 
 // ------------------------------------------------------------------ row pass
@@ -193,10 +193,11 @@ PassArgs<T> l1d_args(const FftOperator<T>& op, bool row, double scale, const int
 template <typename T, typename TS>
 cudaError_t l1d_first(const FftOperator<T>& op, const TS* src, const int* skip, cudaStream_t st) {
     auto k = l1d_first_kernel<T, TS>;
-    const size_t smem = 2 * (size_t)op.l1Q * L1D_TB * sizeof(cplx_t<T>);
+    const size_t smem = 2 * (size_t)op.l1Q * op.l1TB * sizeof(cplx_t<T>);
     cudaError_t e = smem_optin(k, smem);
     if (e != cudaSuccess) return e;
-    k<<<(op.l1P + L1D_TB - 1) / L1D_TB, 256, smem, st>>>(l1d_args(op, false, 1.0, skip), src, op.tw1, op.l1P, op.l1Q);
+    k<<<(op.l1P + op.l1TB - 1) / op.l1TB, 256, smem, st>>>(l1d_args(op, false, 1.0, skip), src, op.tw1, op.l1P,
+                                                            op.l1Q, op.l1TB);
     return cudaGetLastError();
 }
 

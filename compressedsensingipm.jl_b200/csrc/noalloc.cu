@@ -98,8 +98,7 @@ int csipm_apply_AtA_static(int dim, const int* size, const uint32_t* keep_bits, 
             !make_fft_plan(op.l1Q, &op.planQ, &err, op.max_radix()))
             return static_fail(CSIPM_ERR_UNSUPPORTED, err);
         if (!op.choose_strided(op.planQ, op.l1Q, op.l1P, 1, &op.q_cfg, &err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);
-        op.l1RB = 1;
-        while (op.l1RB < 16 && 2 * (size_t)op.l1P * (2 * op.l1RB) * sizeof(C) <= 96 * 1024) op.l1RB *= 2;
+        l1d_tiles(op.l1P, op.l1Q, sizeof(C), &op.l1TB, &op.l1RB);
         op.plan1 = op.planP;
     } else {
         if (!op.make_plans(&err)) return static_fail(CSIPM_ERR_UNSUPPORTED, err);

@@ -630,7 +630,7 @@ inline unsigned mask_blocks(long long n) { return (unsigned)std::max<long long>(
 constexpr int L1D_MIN_M = 2048;
 constexpr int L1D_MAX_P = 4096;     // row length of the four-step row kernel
 constexpr int L1D_MAX_Q = 768;      // line length of the first and last passes
-constexpr int L1D_TB = 8;           // lines per CTA of the first pass
+constexpr int L1D_TB = 8;           // most lines per CTA of the first pass
 
 // M = P*Q with Q the largest divisor of M not above sqrt(M) (nor L1D_MAX_Q),
 // P = M/Q; false when P exceeds L1D_MAX_P
@@ -682,6 +682,22 @@ inline cudaError_t launch_twiddles(int L, C* dst, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Lines per CTA of the first pass (TB) and rows per CTA of the row pass (RB):
+// as wide as shared memory allows (TB <= L1D_TB, RB <= 16) while each pass
+// still launches about one CTA per SM (148 on B200; 128 for FP64, whose wide
+// tiles measured faster down to that count).  A long row has only P and Q
+// lines (a few hundred to a few thousand), so the widest tiles left most SMs
+// idle (2^17: 32 CTAs per pass); the tile width changes no arithmetic.
+inline void l1d_tiles(int P, int Q, size_t csize, int* TB, int* RB) {
+    const int TARGET = csize >= 16 ? 128 : 148;
+    int tb = L1D_TB;
+    while (tb > 2 && (P + tb - 1) / tb < TARGET) tb /= 2;
+    int rb = 1;
+    while (rb < 16 && 2 * (size_t)P * (2 * rb) * csize <= 96 * 1024 && Q / (2 * rb) >= TARGET) rb *= 2;
+    *TB = tb;
+    *RB = rb;
+}
+
 template <typename T>
 class FftOperator {
 public:
@@ -702,7 +718,7 @@ public:
     bool owns = true;               // false: buffers belong to someone else; release() frees nothing
     const int4* pmap = nullptr;     // solver-order plane map (owned by the handle)
     // long 1D rows: M = l1P * l1Q (0 when the one-CTA row pass is used)
-    int l1P = 0, l1Q = 0, l1RB = 0;
+    int l1P = 0, l1Q = 0, l1RB = 0, l1TB = 0;
     FftPlanDev planP{}, planQ{};
     C* twP = nullptr;
     C* twQ = nullptr;
@@ -850,8 +866,7 @@ public:
             if (!make_fft_plan(l1P, &planP, err, max_radix()) || !make_fft_plan(l1Q, &planQ, err, max_radix()))
                 return false;
             if (!choose_strided(planQ, l1Q, l1P, 1, &q_cfg, err)) return false;
-            l1RB = 1;
-            while (l1RB < 16 && 2 * (size_t)l1P * (2 * l1RB) * sizeof(C) <= 96 * 1024) l1RB *= 2;
+            l1d_tiles(l1P, l1Q, sizeof(C), &l1TB, &l1RB);
             if (!upload_table(l1P, &twP, err) || !upload_table(l1Q, &twQ, err)) return false;
             plan1 = planP;   // unused by the long path; keeps the handle's plans defined
         } else {
