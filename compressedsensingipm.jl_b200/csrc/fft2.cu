@@ -50,7 +50,7 @@ cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st) {
         row2_kernel<T, AA, BB, IN, OUT, MASK><<<grid, Sh::ROWS * Sh::NTL, 0, st>>>(a);                     \
         return cudaGetLastError();                                                                         \
     }
-    CSIPM_R2(10, 16) CSIPM_R2(8, 16) CSIPM_R2(8, 10) CSIPM_R2(8, 8) CSIPM_R2(16, 16)
+    CSIPM_R2(10, 16) CSIPM_R2(8, 16) CSIPM_R2(8, 10) CSIPM_R2(8, 8) CSIPM_R2(16, 16) CSIPM_R2(16, 32)
 #undef CSIPM_R2
     return cudaErrorInvalidValue;
 }

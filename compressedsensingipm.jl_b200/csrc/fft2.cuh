@@ -601,10 +601,10 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
 }
 
 // --------------------------------------------------------------- dispatch
-// Factor L = A*B for the two-level passes (A, B <= 20, A <= B, balanced);
+// Factor L = A*B for the two-level passes (A, B in {4..20, 32}, A <= B, balanced);
 // returns false when L has no supported factorisation.
 inline bool fft2_factor(int L, int* A, int* B) {
-    static const int sup[] = {20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
+    static const int sup[] = {32, 20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
     int bestA = 0, bestB = 0;
     for (int b : sup) {
         if (L % b) continue;
@@ -627,7 +627,7 @@ inline bool fft2_strided_pair(int A, int B) {
 }
 inline bool fft2_row_pair(int A, int B) {
     return (A == 10 && B == 16) || (A == 8 && B == 16) || (A == 8 && B == 10) || (A == 8 && B == 8) ||
-           (A == 16 && B == 16);
+           (A == 16 && B == 16) || (A == 16 && B == 32);
 }
 
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
