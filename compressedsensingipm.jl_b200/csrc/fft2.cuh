@@ -620,14 +620,24 @@ inline bool fft2_factor(int L, int* A, int* B) {
     return true;
 }
 
-// The (A, B) pairs the library instantiates (fft2.cu).
+// The (A, B) pairs the library instantiates (fft2_*.cu): the lengths of the
+// 320^3 / 256^3 / 2D 1024^2 workloads and the common dimension lengths of
+// 3D recoveries with sides of 32-128 samples and factors 2, 3, 5.
+#define CSIPM_FFT2_SPAIRS(X) \
+    X(16, 20) X(16, 16) X(10, 16) X(8, 16) X(8, 8) X(10, 12) X(9, 12) X(8, 10) X(8, 9) X(9, 10) X(10, 10) \
+    X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8)
+#define CSIPM_FFT2_RPAIRS(X) \
+    X(10, 16) X(8, 16) X(8, 10) X(8, 8) X(16, 16) X(16, 32) X(6, 10) X(6, 6) X(6, 9) X(5, 10) X(4, 8) \
+    X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5)
 inline bool fft2_strided_pair(int A, int B) {
-    return (A == 16 && B == 20) || (A == 16 && B == 16) || (A == 10 && B == 16) || (A == 8 && B == 16) ||
-           (A == 8 && B == 8);
+#define CSIPM_IS_PAIR(AA, BB) if (A == AA && B == BB) return true;
+    CSIPM_FFT2_SPAIRS(CSIPM_IS_PAIR)
+    return false;
 }
 inline bool fft2_row_pair(int A, int B) {
-    return (A == 10 && B == 16) || (A == 8 && B == 16) || (A == 8 && B == 10) || (A == 8 && B == 8) ||
-           (A == 16 && B == 16) || (A == 16 && B == 32);
+    CSIPM_FFT2_RPAIRS(CSIPM_IS_PAIR)
+#undef CSIPM_IS_PAIR
+    return false;
 }
 
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
@@ -638,7 +648,7 @@ cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st);
 
 // The instantiations of the two-level passes (fft2.cu): (T, INV, IN, OUT, TS,
 // Epi) and (T, IN, OUT, MASK).  Fft2S / Fft2R tell the dispatch which exist.
-#define CSIPM_FFT2_STRIDED_LIST(X)                                   \
+#define CSIPM_FFT2_STRIDED_LIST64(X)                                 \
     X(double, true, IN_GATHER, OUT_SPEC, double, EpiStore<double>)   \
     X(double, true, IN_SPEC, OUT_SPEC, double, EpiStore<double>)     \
     X(double, false, IN_SPEC, OUT_SPEC, double, EpiStore<double>)    \
@@ -646,22 +656,26 @@ cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st);
     X(double, false, IN_SPEC, OUT_SCATTER, double, EpiCG<double>)    \
     X(double, true, IN_SGATHER, OUT_SPEC, double, EpiStore<double>)  \
     X(double, false, IN_SPEC, OUT_SSCATTER, double, EpiStore<double>) \
-    X(double, false, IN_SPEC, OUT_SSCATTER, double, EpiCG<double>)   \
+    X(double, false, IN_SPEC, OUT_SSCATTER, double, EpiCG<double>)
+#define CSIPM_FFT2_STRIDED_LIST32(X)                                 \
     X(float, true, IN_GATHER, OUT_SPEC, float, EpiStore<double>)     \
     X(float, true, IN_SGATHER, OUT_SPEC, float, EpiStore<double>)    \
     X(float, true, IN_SPEC, OUT_SPEC, double, EpiStore<double>)      \
     X(float, false, IN_SPEC, OUT_SPEC, double, EpiStore<double>)     \
     X(float, false, IN_SPEC, OUT_SCATTER, double, EpiCG<float>)      \
     X(float, false, IN_SPEC, OUT_SSCATTER, double, EpiCG<float>)
+#define CSIPM_FFT2_STRIDED_LIST(X) CSIPM_FFT2_STRIDED_LIST64(X) CSIPM_FFT2_STRIDED_LIST32(X)
 
-#define CSIPM_FFT2_ROW_LIST(X)           \
+#define CSIPM_FFT2_ROW_LIST64(X)         \
     X(double, IN_SPEC, OUT_SPEC, true)   \
     X(double, IN_SPEC, OUT_SPEC, false)  \
     X(double, IN_SPEC, OUT_REAL, true)   \
     X(double, IN_SPEC, OUT_REAL, false)  \
-    X(double, IN_REAL, OUT_SPEC, false)  \
+    X(double, IN_REAL, OUT_SPEC, false)
+#define CSIPM_FFT2_ROW_LIST32(X)         \
     X(float, IN_SPEC, OUT_SPEC, true)    \
     X(float, IN_SPEC, OUT_SPEC, false)
+#define CSIPM_FFT2_ROW_LIST(X) CSIPM_FFT2_ROW_LIST64(X) CSIPM_FFT2_ROW_LIST32(X)
 
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
 struct Fft2S { static constexpr bool value = false; };

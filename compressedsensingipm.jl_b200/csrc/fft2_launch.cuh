@@ -1,5 +1,8 @@
-// Instantiations and launchers of the two-level register FFT passes
-// (fft2.cuh) for the line lengths the library runs them on.
+// Launchers of the two-level register FFT passes (fft2.cuh): dispatch on the
+// factor pair to the kernel instantiated for it.  The explicit
+// instantiations are split over fft2_s64.cu, fft2_s32.cu, fft2_r64.cu and
+// fft2_r32.cu so they compile in parallel.
+#pragma once
 #include "fft2.cuh"
 
 namespace csipm {
@@ -13,7 +16,7 @@ cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, c
         strided2_kernel<T, AA, BB, INV, IN, OUT, TS, Epi><<<grid, TB * (AA > BB ? AA : BB), 0, st>>>(a, src, epi); \
         return cudaGetLastError();                                                                         \
     }
-    CSIPM_S2(16, 20) CSIPM_S2(16, 16) CSIPM_S2(10, 16) CSIPM_S2(8, 16) CSIPM_S2(8, 8)
+    CSIPM_FFT2_SPAIRS(CSIPM_S2)
 #undef CSIPM_S2
     return cudaErrorInvalidValue;
 }
@@ -50,19 +53,9 @@ cudaError_t launch_row2(int A, int B, const PassArgs<T>& a, cudaStream_t st) {
         row2_kernel<T, AA, BB, IN, OUT, MASK><<<grid, Sh::ROWS * Sh::NTL, 0, st>>>(a);                     \
         return cudaGetLastError();                                                                         \
     }
-    CSIPM_R2(10, 16) CSIPM_R2(8, 16) CSIPM_R2(8, 10) CSIPM_R2(8, 8) CSIPM_R2(16, 16) CSIPM_R2(16, 32)
+    CSIPM_FFT2_RPAIRS(CSIPM_R2)
 #undef CSIPM_R2
     return cudaErrorInvalidValue;
 }
-
-#define CSIPM_INST_S2(T, INV, IN, OUT, TS, EPI) \
-    template cudaError_t launch_strided2<T, INV, IN, OUT, TS, EPI>(int, int, const PassArgs<T>&, const TS*, const EPI&, cudaStream_t);
-CSIPM_FFT2_STRIDED_LIST(CSIPM_INST_S2)
-#undef CSIPM_INST_S2
-
-#define CSIPM_INST_R2(T, IN, OUT, MASK) \
-    template cudaError_t launch_row2<T, IN, OUT, MASK>(int, int, const PassArgs<T>&, cudaStream_t);
-CSIPM_FFT2_ROW_LIST(CSIPM_INST_R2)
-#undef CSIPM_INST_R2
 
 }  // namespace csipm

@@ -39,7 +39,8 @@ def _problem(kind, dims, seed):
 
 @pytest.mark.parametrize("kind,dims", [("1d", (2048,)), ("1d", (16384,)), ("2d", (64, 64)), ("2d", (128, 96)),
                                        ("2d", (96, 128)), ("3d", (16, 16, 16)), ("3d", (32, 32, 32)),
-                                       ("3d", (32, 64, 24)), ("3d", (64, 64, 64))])
+                                       ("3d", (32, 64, 24)), ("3d", (64, 64, 64)), ("3d", (60, 48, 40)),
+                                       ("3d", (72, 90, 54))])
 def test_parity_with_cpu_twin(cuda, kind, dims):
     """Same seed, same algorithm: beta within 1e-6 relative, objective within
     1e-8 relative, IPM iteration count within 1."""

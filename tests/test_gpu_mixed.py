@@ -30,7 +30,7 @@ def _solve(torch, prob, precision, **kw):
 # solver order (second dimension 64/128/160/256/320) and reference order
 # (Stockham FP32 passes), 1D row passes
 @pytest.mark.parametrize("kind,dims", [("1d", (4096,)), ("1d", (24000,)), ("2d", (64, 64)), ("2d", (96, 128)), ("3d", (32, 32, 32)),
-                                       ("3d", (32, 64, 24)), ("3d", (64, 64, 64))])
+                                       ("3d", (32, 64, 24)), ("3d", (64, 64, 64)), ("3d", (40, 60, 36))])
 @pytest.mark.parametrize("cg_rtol", [1e-8, 1e-5, 1e-2])
 def test_mixed_matches_fp64(cuda, kind, dims, cg_rtol):
     """1e-2 runs the loose mode: FP32 Newton directions, corrector warm start

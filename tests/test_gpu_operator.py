@@ -13,6 +13,11 @@ TOL = 1e-12
 # 1D rows above 4096 samples take the multi-CTA four-step path (M = P*Q)
 EXTRA = [(16384,), (1000,), (2 * 3 * 5 * 7 * 2,), (256, 256), (62, 82), (30, 42), (64, 64, 64), (32, 48, 40),
          (14, 22, 26), (20, 30, 18), (8192,), (4374,), (2 * 2 * 3 * 5 * 7 * 11,), (24000,), (65536,), (2 ** 20,)]
+# every two-level factor pair of the strided passes (dims 2, 3) and of the
+# row pass (dim 1: M = N1/2) that serves sides of 32-128 with factors 2, 3, 5
+PAIR_GRID = [(120, 108, 80), (72, 72, 90), (108, 100, 96), (100, 40, 48), (64, 54, 36), (90, 60, 50),
+             (80, 32, 120), (48, 96, 40), (96, 50, 54), (40, 36, 60), (60, 72, 32), (50, 90, 100), (120, 108),
+             (90, 100)]
 
 
 def relerr(a, b):
@@ -32,7 +37,7 @@ def make_op(size, keep, rdft=True):
     return csipm.FFTOperator(params, rdft=rdft), z0
 
 
-@pytest.mark.parametrize("size", REF_GRID + EXTRA)
+@pytest.mark.parametrize("size", REF_GRID + EXTRA + PAIR_GRID)
 @pytest.mark.parametrize("masked", [False, True])
 def test_operator_matches_oracle(cuda, size, masked):
     torch = cuda
