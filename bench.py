@@ -76,7 +76,9 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=16, help="concurrent solves of the serving loop")
     ap.add_argument("--serve-batch", type=int, default=32,
                     help="requests of one batch class a slot solves together in the batched closed run (<= 1: skip)")
-    ap.add_argument("--serve-batch-slots", type=int, default=8, help="slots of the batched closed run")
+    ap.add_argument("--serve-batch-slots", type=int, default=16, help="slots of the batched closed run")
+    ap.add_argument("--serve-batch-max-n", type=int, default=1 << 16,
+                    help="batched closed run: requests of more samples are solved alone (0: no limit)")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving leg and print its JSON object (slot-count experiments)")
     ap.add_argument("--no-graphs", action="store_true",
@@ -689,12 +691,12 @@ def run_serving(args, n_req, slots, rank):
     seq_plain_rate, seq_plain_failed, seq_plain_share = sequential(dict(opts, cuda_graphs=False))
     seq_rate = max(seq_graph_rate, seq_plain_rate)
 
-    def serve(rate, graphs, batch=1, nslots=slots):
+    def serve(rate, graphs, batch=1, nslots=slots, batch_max_n=0):
         rng = np.random.default_rng(7)
         gaps = rng.exponential(1.0 / rate, size=n_req) if rate else np.zeros(n_req)
         arrivals = np.cumsum(gaps) - gaps[0]
         res = []
-        with Server(slots=nslots, cuda_graphs=graphs, batch=batch) as srv:
+        with Server(slots=nslots, cuda_graphs=graphs, batch=batch, batch_max_n=batch_max_n) as srv:
             t_start = time.perf_counter()
             for k, r in enumerate(reqs):
                 while True:
@@ -722,6 +724,7 @@ def run_serving(args, n_req, slots, rank):
     # running service)
     batch = int(getattr(args, "serve_batch", 1))
     bslots = int(getattr(args, "serve_batch_slots", slots))
+    bmax = int(getattr(args, "serve_batch_max_n", 0))
     for warm_batch, warm_slots in (((1, slots), (batch, bslots)) if batch > 1 else ((1, slots),)):
         with Server(slots=warm_slots, batch=warm_batch) as srv:
             for k, r in enumerate(reqs[:max(warm_slots, 4 * warm_batch)]):
@@ -735,15 +738,15 @@ def run_serving(args, n_req, slots, rank):
         # one-at-a-time modes are warm from the sequential runs: every kernel
         # loaded, the memory pool grown to what their peak holds; batches hold
         # more handles at once)
-        serve(0.0, False, batch, bslots)
-        closed_batched = serve(0.0, False, batch, bslots)
+        serve(0.0, False, batch, bslots, bmax)
+        closed_batched = serve(0.0, False, batch, bslots, bmax)
     # the fastest closed mode sets the Poisson run's mode and offered rate
-    modes = [(closed_plain, False, 1, slots), (closed_graphs, True, 1, slots)]
+    modes = [(closed_plain, False, 1, slots, 0), (closed_graphs, True, 1, slots, 0)]
     if closed_batched:
-        modes.append((closed_batched, False, batch, bslots))
-    closed, graphs, pbatch, pslots = max(modes, key=lambda m: m[0]["solves_per_s"])
+        modes.append((closed_batched, False, batch, bslots, bmax))
+    closed, graphs, pbatch, pslots, pbmax = max(modes, key=lambda m: m[0]["solves_per_s"])
     offered = 0.8 * closed["solves_per_s"]
-    poisson = serve(offered, graphs, pbatch, pslots)
+    poisson = serve(offered, graphs, pbatch, pslots, pbmax)
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("1d", "2d", "3d")}
     return {
         "requests": n_req, "slots": slots, "mix": kinds,
@@ -759,9 +762,10 @@ def run_serving(args, n_req, slots, rank):
         "batched_closed": dict(closed, cuda_graphs=graphs, batch=pbatch, slots=pslots),
         "batched_closed_plain_launches": closed_plain,
         "batched_closed_graph_launches": closed_graphs,
-        "batched_closed_solve_batch": (dict(closed_batched, batch=batch, slots=bslots,
+        "batched_closed_solve_batch": (dict(closed_batched, batch=batch, slots=bslots, batch_max_n=bmax,
                                             what="each slot solves up to `batch` admitted requests of one batch "
-                                                 "class together (csipm_solve_batch, FP64)")
+                                                 "class together (csipm_solve_batch, FP64); requests above "
+                                                 "batch_max_n samples alone")
                                        if closed_batched else None),
         "batched_poisson": dict(poisson, offered_per_s=round(offered, 2), cuda_graphs=graphs, batch=pbatch,
                                 slots=pslots),
