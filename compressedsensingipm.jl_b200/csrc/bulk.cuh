@@ -1,6 +1,6 @@
 // Bulk asynchronous copies global -> shared (the TMA engine without a tensor
 // map: cp.async.bulk) and the mbarriers that count their bytes, for sm_100a.
-// CTA-local only: no cluster multicast anywhere.
+// CTA-local copies only: each CTA fetches its own tiles.
 #pragma once
 #include <cstdint>
 
