@@ -966,8 +966,9 @@ int csipm_create(const csipm_problem* prob, const csipm_options* opt_in, csipm_h
     }
     // reduction workspace: enough partials for the largest grid
     size_t maxblocks = 8192;
-    if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * (h->g.dim == 3 ? h->g.n3 : 1));
-    if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB) / FFT2_TB) * h->g.n2);
+    if (h->g.dim >= 2)
+        maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB_MIN) / FFT2_TB_MIN) * (h->g.dim == 3 ? h->g.n3 : 1));
+    if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)((h->g.m1 + FFT2_TB_MIN) / FFT2_TB_MIN) * h->g.n2);
     maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.row_cfg.grid.x);
     if (h->g.dim >= 2) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s2_cfg.grid.x * h->op64.s2_cfg.grid.y);
     if (h->g.dim >= 3) maxblocks = std::max<size_t>(maxblocks, (size_t)h->op64.s3_cfg.grid.x * h->op64.s3_cfg.grid.y);

@@ -20,9 +20,17 @@
 
 namespace csipm {
 
-// lines per CTA of the strided two-level pass: 128 B per access (8 FP64 or 16 FP32 complex)
-constexpr int FFT2_TB = 8;
-template <typename T> constexpr int fft2_tb() { return sizeof(T) == 8 ? 8 : 16; }
+// Lines per CTA of the strided two-level pass of length L: 128 B per access
+// (8 FP64 or 16 FP32 complex) while the CTA's lines fit the 48 KB of static
+// shared memory, else the most that fit (lines above 384 points: 4 or 2).
+template <typename T, int L> constexpr int fft2_tb() {
+    constexpr int full = sizeof(T) == 8 ? 8 : 16;
+    constexpr int fit = (48 * 1024) / (L * 2 * (int)sizeof(T));
+    return fit >= full ? full : (fit >= 8 ? 8 : (fit >= 4 ? 4 : 2));
+}
+// fewest lines per CTA of any strided two-level pass (sizes the grid-reduction
+// workspace of the scatter passes, whose grids have (N1/2+1)/TB columns)
+constexpr int FFT2_TB_MIN = 2;
 
 // twiddle of the strided pass: W_L^e (forward) from a table of L-th roots
 template <bool INV, typename C>
@@ -48,12 +56,12 @@ template <typename T, int IN, int OUT, int NT> constexpr int fft2_min_ctas() {
 }
 
 template <typename T, int A, int B, bool INV, int IN, int OUT, typename TS, class Epi>
-__global__ void __launch_bounds__(fft2_tb<T>() * (A > B ? A : B),
-                                  (fft2_min_ctas<T, IN, OUT, fft2_tb<T>() * (A > B ? A : B)>()))
+__global__ void __launch_bounds__(fft2_tb<T, A * B>() * (A > B ? A : B),
+                                  (fft2_min_ctas<T, IN, OUT, fft2_tb<T, A * B>() * (A > B ? A : B)>()))
 strided2_kernel(PassArgs<T> a, const TS* __restrict__ src, Epi epi) {
     using C = cplx_t<T>;
-    constexpr int TB = fft2_tb<T>();
     constexpr int L = A * B;
+    constexpr int TB = fft2_tb<T, L>();
     if (a.skip && *a.skip) return;
     __shared__ C S[L * TB];
     const int b = threadIdx.x % TB, t = threadIdx.x / TB;
@@ -621,11 +629,12 @@ inline bool fft2_factor(int L, int* A, int* B) {
 }
 
 // The (A, B) pairs the library instantiates (fft2_*.cu): the lengths of the
-// 320^3 / 256^3 / 2D 1024^2 workloads and the common dimension lengths of
+// 320^3 / 256^3 / 2D 1024^2 workloads (strided 1024 = 32 x 32 at 2 FP64 or
+// 4 FP32 lines per CTA) and the common dimension lengths of
 // 3D recoveries with sides of 32-128 samples and factors 2, 3, 5.
 #define CSIPM_FFT2_SPAIRS(X) \
     X(16, 20) X(16, 16) X(10, 16) X(8, 16) X(8, 8) X(10, 12) X(9, 12) X(8, 10) X(8, 9) X(9, 10) X(10, 10) \
-    X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8)
+    X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8) X(32, 32)
 #define CSIPM_FFT2_RPAIRS(X) \
     X(10, 16) X(8, 16) X(8, 10) X(8, 8) X(16, 16) X(16, 32) X(6, 10) X(6, 6) X(6, 9) X(5, 10) X(4, 8) \
     X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5)

@@ -9,10 +9,10 @@ namespace csipm {
 
 template <typename T, bool INV, int IN, int OUT, typename TS, class Epi>
 cudaError_t launch_strided2(int A, int B, const PassArgs<T>& a, const TS* src, const Epi& epi, cudaStream_t st) {
-    constexpr int TB = fft2_tb<T>();
-    const dim3 grid((a.n_lines + TB - 1) / TB, a.n_outer, 1);
 #define CSIPM_S2(AA, BB)                                                                                   \
     if (A == AA && B == BB) {                                                                              \
+        constexpr int TB = fft2_tb<T, AA * BB>();                                                          \
+        const dim3 grid((a.n_lines + TB - 1) / TB, a.n_outer, 1);                                          \
         strided2_kernel<T, AA, BB, INV, IN, OUT, TS, Epi><<<grid, TB * (AA > BB ? AA : BB), 0, st>>>(a, src, epi); \
         return cudaGetLastError();                                                                         \
     }
