@@ -612,7 +612,7 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
 // Factor L = A*B for the two-level passes (A, B in {4..20, 32}, A <= B, balanced);
 // returns false when L has no supported factorisation.
 inline bool fft2_factor(int L, int* A, int* B) {
-    static const int sup[] = {32, 20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
+    static const int sup[] = {32, 25, 20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
     int bestA = 0, bestB = 0;
     for (int b : sup) {
         if (L % b) continue;
@@ -630,14 +630,17 @@ inline bool fft2_factor(int L, int* A, int* B) {
 
 // The (A, B) pairs the library instantiates (fft2_*.cu): the lengths of the
 // 320^3 / 256^3 / 2D 1024^2 workloads (strided 1024 = 32 x 32 at 2 FP64 or
-// 4 FP32 lines per CTA) and the common dimension lengths of
-// 3D recoveries with sides of 32-128 samples and factors 2, 3, 5.
+// 4 FP32 lines per CTA) and the common dimension lengths of the serving
+// stream's recoveries (3D sides of 32-128, 2D sides of 128-1024, factors
+// 2, 3, 5), picked from its length histogram weighted by work (pairs whose
+// kernels would spill registers heavily are left to Stockham).
 #define CSIPM_FFT2_SPAIRS(X) \
     X(16, 20) X(16, 16) X(10, 16) X(8, 16) X(8, 8) X(10, 12) X(9, 12) X(8, 10) X(8, 9) X(9, 10) X(10, 10) \
-    X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8) X(32, 32)
+    X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8) X(32, 32) X(20, 20) X(25, 32) \
+    X(15, 16) X(15, 20) X(12, 15) X(20, 25)
 #define CSIPM_FFT2_RPAIRS(X) \
     X(10, 16) X(8, 16) X(8, 10) X(8, 8) X(16, 16) X(16, 32) X(6, 10) X(6, 6) X(6, 9) X(5, 10) X(4, 8) \
-    X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5)
+    X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5) X(12, 15) X(15, 32) X(15, 15) X(4, 4) X(15, 20)
 inline bool fft2_strided_pair(int A, int B) {
 #define CSIPM_IS_PAIR(AA, BB) if (A == AA && B == BB) return true;
     CSIPM_FFT2_SPAIRS(CSIPM_IS_PAIR)

@@ -14,10 +14,12 @@ TOL = 1e-12
 EXTRA = [(16384,), (1000,), (2 * 3 * 5 * 7 * 2,), (256, 256), (62, 82), (30, 42), (64, 64, 64), (32, 48, 40),
          (14, 22, 26), (20, 30, 18), (8192,), (4374,), (2 * 2 * 3 * 5 * 7 * 11,), (24000,), (65536,), (2 ** 20,)]
 # every two-level factor pair of the strided passes (dims 2, 3) and of the
-# row pass (dim 1: M = N1/2) that serves sides of 32-128 with factors 2, 3, 5
+# row pass (dim 1: M = N1/2) that serves the 3D sides of 32-128 and the 2D
+# sides of 128-1024 with factors 2, 3, 5
 PAIR_GRID = [(120, 108, 80), (72, 72, 90), (108, 100, 96), (100, 40, 48), (64, 54, 36), (90, 60, 50),
              (80, 32, 120), (48, 96, 40), (96, 50, 54), (40, 36, 60), (60, 72, 32), (50, 90, 100), (120, 108),
-             (90, 100)]
+             (90, 100), (360, 400), (960, 240), (450, 300), (600, 180), (360, 500), (960, 800), (32, 36, 40),
+             (1024, 1024)]
 
 
 def relerr(a, b):
