@@ -88,3 +88,18 @@ def test_batch_rejects_mixed_kinds(cuda):
     with pytest.raises(_native.CsipmError) as e:
         csipm.ipm_solve_batch([m2, m3])
     assert e.value.status == _native.CSIPM_ERR_INVALID
+
+
+def test_batch_takes_mixed_precision_handles(cuda):
+    """Handles created for mixed precision join a batch and are solved on its
+    FP64 path: each result equals the FP64 solve alone (beta within 1e-6)."""
+    import csipm
+    torch = cuda
+    probs = [_problem("3d", (32, 32, 32), seed=51), _problem("3d", (40, 36, 48), seed=52)]
+    opts = dict(tol=1e-10, ipm_cg_rtol=1e-2)
+    batch = csipm.ipm_solve_batch([_model(torch, p, precision="mixed", **opts) for p in probs])
+    for prob, res in zip(probs, batch):
+        assert res.status == 0, res.stats
+        alone = csipm.ipm_solve(_model(torch, prob, precision="fp64", **opts))
+        b, a = res.beta.cpu().numpy(), alone.beta.cpu().numpy()
+        assert np.linalg.norm(b - a) / np.linalg.norm(a) <= 1e-6
