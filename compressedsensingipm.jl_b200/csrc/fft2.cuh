@@ -25,7 +25,7 @@ namespace csipm {
 // shared memory, else the most that fit (lines above 384 points: 4 or 2).
 template <typename T, int L> constexpr int fft2_tb() {
     constexpr int full = sizeof(T) == 8 ? 8 : 16;
-    constexpr int fit = (48 * 1024) / (L * 2 * (int)sizeof(T));
+    constexpr int fit = (47 * 1024) / (L * 2 * (int)sizeof(T));   // 1 KB left for the reductions' arrays
     return fit >= full ? full : (fit >= 8 ? 8 : (fit >= 4 ? 4 : 2));
 }
 // fewest lines per CTA of any strided two-level pass (sizes the grid-reduction
@@ -609,10 +609,10 @@ row2b_kernel(PassArgs<T> a, int ntiles) {
 }
 
 // --------------------------------------------------------------- dispatch
-// Factor L = A*B for the two-level passes (A, B in {4..20, 32}, A <= B, balanced);
+// Factor L = A*B for the two-level passes (A, B among the register DFT sizes, A <= B, balanced);
 // returns false when L has no supported factorisation.
 inline bool fft2_factor(int L, int* A, int* B) {
-    static const int sup[] = {32, 25, 20, 16, 15, 12, 10, 9, 8, 6, 5, 4};
+    static const int sup[] = {32, 30, 27, 25, 24, 20, 18, 16, 15, 12, 10, 9, 8, 6, 5, 4};
     int bestA = 0, bestB = 0;
     for (int b : sup) {
         if (L % b) continue;
@@ -633,14 +633,17 @@ inline bool fft2_factor(int L, int* A, int* B) {
 // 4 FP32 lines per CTA) and the common dimension lengths of the serving
 // stream's recoveries (3D sides of 32-128, 2D sides of 128-1024, factors
 // 2, 3, 5), picked from its length histogram weighted by work (pairs whose
-// kernels would spill registers heavily are left to Stockham).
+// kernels spill registers heavily, or that the autotuner found slower than
+// Stockham, are left to Stockham).
 #define CSIPM_FFT2_SPAIRS(X) \
     X(16, 20) X(16, 16) X(10, 16) X(8, 16) X(8, 8) X(10, 12) X(9, 12) X(8, 10) X(8, 9) X(9, 10) X(10, 10) \
     X(8, 12) X(5, 8) X(6, 8) X(6, 9) X(6, 6) X(6, 10) X(5, 10) X(4, 8) X(32, 32) X(20, 20) X(25, 32) \
-    X(15, 16) X(15, 20) X(12, 15) X(20, 25)
+    X(15, 16) X(15, 20) X(12, 15) X(20, 25) X(27, 32) X(18, 24) X(30, 32) X(24, 24) X(30, 30) X(24, 25) \
+    X(18, 18) X(18, 20) X(27, 30)
 #define CSIPM_FFT2_RPAIRS(X) \
     X(10, 16) X(8, 16) X(8, 10) X(8, 8) X(16, 16) X(16, 32) X(6, 10) X(6, 6) X(6, 9) X(5, 10) X(4, 8) \
-    X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5) X(12, 15) X(15, 32) X(15, 15) X(4, 4) X(15, 20)
+    X(5, 9) X(5, 8) X(4, 6) X(6, 8) X(4, 5) X(5, 6) X(5, 5) X(12, 15) X(15, 15) X(4, 4) X(15, 20) \
+    X(18, 20) X(18, 25) X(18, 18) X(9, 18) X(20, 24) X(15, 18) X(12, 18) X(16, 18) X(10, 20) X(16, 20)
 inline bool fft2_strided_pair(int A, int B) {
 #define CSIPM_IS_PAIR(AA, BB) if (A == AA && B == BB) return true;
     CSIPM_FFT2_SPAIRS(CSIPM_IS_PAIR)

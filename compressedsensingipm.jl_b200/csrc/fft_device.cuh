@@ -195,6 +195,10 @@ template <bool INV, typename T> struct Dft<16, INV, T> : DftComp<4, 4, INV, T> {
 template <bool INV, typename T> struct Dft<20, INV, T> : DftComp<4, 5, INV, T> {};
 template <bool INV, typename T> struct Dft<25, INV, T> : DftComp<5, 5, INV, T> {};
 template <bool INV, typename T> struct Dft<32, INV, T> : DftComp<8, 4, INV, T> {};
+template <bool INV, typename T> struct Dft<18, INV, T> : DftComp<2, 9, INV, T> {};
+template <bool INV, typename T> struct Dft<24, INV, T> : DftComp<8, 3, INV, T> {};
+template <bool INV, typename T> struct Dft<27, INV, T> : DftComp<3, 9, INV, T> {};
+template <bool INV, typename T> struct Dft<30, INV, T> : DftComp<5, 6, INV, T> {};
 
 // ------------------------------------------------------------------- stages
 template <typename T, int R, bool INV>

@@ -19,7 +19,8 @@ EXTRA = [(16384,), (1000,), (2 * 3 * 5 * 7 * 2,), (256, 256), (62, 82), (30, 42)
 PAIR_GRID = [(120, 108, 80), (72, 72, 90), (108, 100, 96), (100, 40, 48), (64, 54, 36), (90, 60, 50),
              (80, 32, 120), (48, 96, 40), (96, 50, 54), (40, 36, 60), (60, 72, 32), (50, 90, 100), (120, 108),
              (90, 100), (360, 400), (960, 240), (450, 300), (600, 180), (360, 500), (960, 800), (32, 36, 40),
-             (1024, 1024)]
+             (1024, 1024), (720, 864), (900, 432), (648, 960), (324, 576), (960, 900), (540, 600), (432, 324),
+             (576, 360), (400, 810), (864, 256), (640, 128)]
 
 
 def relerr(a, b):
